@@ -1,0 +1,333 @@
+"""Benchmark of the plain single-GPU sort path (2^30 uint32 keys).
+
+python bench.py [--gpus N --steps K --warmup W] [--impl mgs|reference]
+
+One step = one in-place sort of 2^30 uint32 keys drawn by the reference's
+DataGenerator ("uniform" over [0, 2^32), seed 2147483647). Per rank:
+  value : keys/s of mgs_sort_device with the keys resident in HBM. Each step's
+          input is restored from a pristine device copy before the step, outside
+          its CUDA-event timed region; inputs (4 GiB) exceed L2 (126 MB).
+  e2e   : keys/s of mgs_sort_host (TanasicSort with one GPU: pinned host
+          buffer, H2D + sort + D2H inside the timed call), wall-clock.
+  roofline: the onesweep pass kernel, algorithmic bytes (read + write of the
+          keys) per launch over its CUDA-event time, against the measured HBM
+          copy bandwidth.
+  cpu_baseline: the reference's CPU sort (the gnu_parallel branch of
+          src/sort_benchmark.cu, compiled from the reference sources into
+          oracle/_ref) on a bounded sample, rank 0 at N=1 only.
+With torchrun (N>1) every rank sorts its own 2^30 keys on its own GPU (the path
+shards into independent partitions; no data-path collective): weak scaling,
+value = all ranks' keys / the slowest rank's time.
+
+--impl reference times the reference's CPU implementation of the path (same
+metric and workload, bounded sample per step) on the host cores; rank 0 only.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+N_KEYS = 1 << 30
+SEED = 2147483647
+METRIC = "sorted keys/s (2^30 uint32, plain single-GPU sort)"
+WORKLOAD = "plain single-GPU sort: 2^30 uint32 keys, reference DataGenerator 'uniform' [0,2^32), seed 2147483647"
+
+
+def load_mgs():
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("mgs", os.path.join(ROOT, "multi-gpu-sorting_b200", "mgs.py"))
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["mgs"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def load_oracle():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    return oracle
+
+
+def measured_hbm_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        return float(json.load(open(p))["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def committed_traffic(kernel: str):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "radix_onesweep_u32.md")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.startswith("traffic_bytes_per_full_launch:"):
+            return float(line.split(":", 1)[1].strip())
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in getattr(self, "lines", []):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        loaded = [s for s in sm if s > 0.5 * (mx or max(sm))] or sm
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_reference_sort(orc, base: np.ndarray, budget_s: float, max_reps: int):
+    """Times the reference's gnu_parallel sort on copies of `base` (bounded)."""
+    threads = orc.ref_num_procs()
+    work = np.empty_like(base)
+    times = []
+    t_end = time.perf_counter() + budget_s
+    for _ in range(max_reps):
+        np.copyto(work, base)
+        times.append(orc.ref_gnu_parallel_sort(work, threads))
+        if time.perf_counter() > t_end:
+            break
+    return base.size / statistics.median(times), threads, times
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    orc = load_oracle()
+    if not orc.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref.so not built"}))
+        return
+    mgs = load_mgs()
+    sample = 1 << 27
+    base = mgs.generate("u32", "uniform", SEED, sample)
+    threads = orc.ref_num_procs()
+    work = np.empty_like(base)
+    for _ in range(args.warmup):
+        np.copyto(work, base)
+        orc.ref_gnu_parallel_sort(work, threads)
+    times = []
+    for _ in range(args.steps):
+        np.copyto(work, base)
+        times.append(orc.ref_gnu_parallel_sort(work, threads))
+    value = sample * len(times) / sum(times)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "keys/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+        "data": "synthetic (reference DataGenerator)",
+        "config": {"workload": WORKLOAD, "sample_keys": sample,
+                   "algorithm": "reference gnu_parallel sort (src/sort_benchmark.cu:314-319), oracle/_ref"},
+        "cpu_baseline": {"value": value, "unit": "keys/s", "cores": threads, "kind": "reference",
+                         "sample": f"2^27 of the 2^30 uint32 keys per step, {args.steps} steps"},
+        "e2e": {"value": value, "unit": "keys/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="mgs", choices=["mgs", "reference"])
+    ap.add_argument("--n", type=int, default=N_KEYS)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local_rank))
+
+    mgs = load_mgs()
+    n = args.n
+    ctx = mgs.Context(local_rank)
+    keys_np = mgs.generate("u32", "uniform", SEED + rank, n)
+    pristine = torch.from_numpy(keys_np.view(np.int32)).cuda()
+    work = torch.empty_like(pristine)
+    temp_bytes = mgs.Context.sort_temp_bytes("u32", n)
+    temp = torch.empty(temp_bytes, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.Stream()
+    sptr = stream.cuda_stream
+
+    def one_sort(timed_events=None):
+        with torch.cuda.stream(stream):
+            work.copy_(pristine)
+            if timed_events is not None:
+                timed_events[0].record(stream)
+            ctx.sort_device(work.data_ptr(), n, "u32", temp.data_ptr(), temp_bytes, sptr)
+            if timed_events is not None:
+                timed_events[1].record(stream)
+
+    for _ in range(args.warmup):
+        one_sort()
+    stream.synchronize()
+    ctx.synchronize()
+
+    # verify the warm-up result: sorted and a permutation (sum + histogram)
+    u = work.to(torch.int64) & 0xFFFFFFFF
+    ok = bool((u[1:] >= u[:-1]).all()) and (u.sum() == (pristine.to(torch.int64) & 0xFFFFFFFF).sum()).item()
+    del u
+
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ctx.launch_count(reset=True)
+    ctx.set_profiling(True)
+    ctx.kernel_times()  # clear
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with ClockSampler(local_rank) as clocks:
+        for i in range(args.steps):
+            one_sort(evs[i])
+        stream.synchronize()
+    torch.cuda.synchronize()
+    launches = ctx.launch_count(reset=True)
+    ktimes = ctx.kernel_times()
+    ctx.set_profiling(False)
+    ctx.synchronize()
+    step_ms = [a.elapsed_time(b) for a, b in evs]
+    total_ms = sum(step_ms)
+    if world > 1:
+        t = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * n * args.steps / (total_ms / 1e3)
+
+    # end to end through the public host API (mgs_sort_host), pinned buffers
+    h = mgs.host_empty(n, np.uint32)
+    e2e_times = []
+    for i in range(args.e2e_steps + 1):
+        np.copyto(h, keys_np)
+        if world > 1:
+            dist.barrier()
+        t0 = time.perf_counter()
+        ctx.sort_host(h)
+        dt = time.perf_counter() - t0
+        if i > 0:  # first call warms the arena
+            e2e_times.append(dt)
+    e2e_ok = bool(np.all(h[1:] >= h[:-1]))
+    e2e_s = sum(e2e_times)
+    if world > 1:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = world * n * len(e2e_times) / e2e_s
+
+    peak, peak_kind = measured_hbm_peak()
+    one = ktimes.get("radix_onesweep", (0, 0.0))
+    hist = ktimes.get("radix_histogram", (0, 0.0))
+    roof = None
+    if one[0] > 0:
+        avg_ms = one[1] / one[0]
+        alg_bytes = 2 * 4 * n  # each pass reads and writes every key
+        achieved = alg_bytes / (avg_ms / 1e3) / 1e9
+        traffic = committed_traffic("radix_onesweep")
+        roof = {"bound": "hbm", "kernel": "radix_onesweep", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                "traffic": traffic, "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_ms}
+    sort_alg_bytes = 36 * n  # 4 passes x (read + write) + one histogram read, 4-byte keys
+    sort_ms = total_ms / args.steps
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        orc = load_oracle()
+        if orc.ref_available():
+            sample = keys_np[: 1 << 27].copy()
+            v, threads, times = cpu_reference_sort(orc, sample, budget_s=15.0, max_reps=5)
+            cpu = {"value": v, "unit": "keys/s", "cores": threads, "kind": "reference",
+                   "sample": f"first 2^27 of the 2^30 keys, {len(times)} runs, median "
+                             f"(reference gnu_parallel sort, src/sort_benchmark.cu:314-319)"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "keys/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": sort_ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32", "data": "synthetic (reference DataGenerator, seeded)",
+            "config": {"workload": WORKLOAD, "keys_per_gpu": n, "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (4 GiB per step)",
+                       "timing": "CUDA events around each sort on its stream; input restored from a pristine "
+                                 "device copy before each step, outside the timed region",
+                       "sort_hbm_alg_gbs": sort_alg_bytes / (sort_ms / 1e3) / 1e9,
+                       "sort_roofline_frac": sort_alg_bytes / (sort_ms / 1e3) / 1e9 / peak,
+                       "verified": ok and e2e_ok},
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": "keys/s", "h2d_bytes_per_step": 4 * n, "d2h_bytes_per_step": 4 * n,
+                    "api": "mgs_sort_host (TanasicSort, one GPU)", "steps": len(e2e_times)},
+            "gpu_launches": launches,
+            "kernel_ms": {k: {"launches": v[0], "total_ms": v[1]} for k, v in ktimes.items()},
+            "clocks": clocks.summary(),
+        }
+        print(json.dumps(line))
+
+    del work, pristine, temp
+    ctx.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

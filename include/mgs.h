@@ -1,0 +1,129 @@
+/*
+ * mgs.h — C ABI of the B200 sort engine (libmgs.so).
+ *
+ * Every entry point returns an int status (MGS_OK on success). A failing call
+ * leaves a human-readable message for the calling thread in
+ * mgs_last_error_string(). No C++ or torch types cross this boundary: keys are
+ * raw bytes described by an mgs_dtype, sizes are counts of keys, streams are
+ * cudaStream_t passed as void*.
+ *
+ * Reference surface replaced (hpides/multi-gpu-sorting, paths inside that
+ * project):
+ *   TanasicSort<T>(HostVector<T>*, gpus)            src/tanasic_sort.cuh:223-299
+ *   SetupTanasicSort(gpus)                          src/tanasic_sort.cuh:206-221
+ *   GowanlockSort<T>(HostVector<T>*, chunk, group,  src/gowanlock_sort.cuh:395-483
+ *                    buffers, gpus)
+ *   SetupGowanlockSort(gpus, threads)               src/gowanlock_sort.cuh:117-125
+ *   thrust::sort(par.on(stream), begin, end)        src/tanasic_sort.cuh:264-266
+ *   thrust::merge(...)                              src/tanasic_sort.cuh:163-167
+ *   SelectPivot / FindPivot                         src/tanasic_sort.cuh:15-87
+ *   __gnu_parallel::multiway_merge(...)             src/gowanlock_sort.cuh:73-74,91-92
+ *   DataGenerator::ComputeDistribution<T>           src/data_generator.cuh:18-36
+ *   HostVector<T> (pinned thrust::host_vector)      src/host_vector.cuh:7
+ *
+ * The reference's CheckCudaError ignores errors in release builds
+ * (src/cuda_error.cuh:5-10); this ABI reports every error as a status.
+ */
+#ifndef MGS_H_
+#define MGS_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define MGS_OK 0
+#define MGS_ERR_INVALID 1   /* bad argument (null pointer, unknown dtype, size limit) */
+#define MGS_ERR_OOM 2       /* device or pinned host allocation failed */
+#define MGS_ERR_CUDA 3      /* a CUDA runtime call failed */
+#define MGS_ERR_TIMEOUT 4   /* a bounded device-side wait gave up (status word set by a kernel) */
+#define MGS_ERR_NO_DEVICE 5 /* no CUDA device, or the device id is out of range */
+#define MGS_ERR_CANCELLED 6 /* a queued request was cancelled before it ran */
+#define MGS_ERR_BUSY 7      /* admission refused: not enough free device memory right now */
+
+/* ---- key types ---------------------------------------------------------
+ * The reference CLI accepts int, long, float, double (src/sort_benchmark.cu:209-221);
+ * the unsigned types are the ones the sort path is benchmarked on. Keys are
+ * sorted ascending in the order thrust::sort / CUB DeviceRadixSort 2.8.2 gives:
+ * signed by value, IEEE-754 by value with -0.0 equal to +0.0 (input order kept,
+ * the sort is stable), NaNs placed by their bit pattern (negative-sign NaNs
+ * before -inf, positive-sign NaNs after +inf). */
+typedef enum mgs_dtype {
+  MGS_U32 = 0,
+  MGS_I32 = 1,
+  MGS_F32 = 2,
+  MGS_U64 = 3,
+  MGS_I64 = 4,
+  MGS_F64 = 5
+} mgs_dtype;
+
+typedef struct mgs_ctx mgs_ctx;
+
+/* ---- library ----------------------------------------------------------- */
+int mgs_version(void);                   /* 10000 * major + 100 * minor + patch */
+const char* mgs_last_error_string(void); /* thread-local; "" when the last call succeeded */
+size_t mgs_dtype_size(int dtype);        /* 4 or 8; 0 for an unknown dtype */
+int mgs_device_count(int* count);
+
+/* ---- context: one per device; owns streams and a grow-only device arena ----
+ * Replaces DeviceBuffers<T> (src/device_buffers.cuh:15-135) and its bump
+ * allocator (src/device_allocator.cuh:10-92): device memory is reserved once
+ * per context instead of per call. arena_bytes == 0 reserves lazily.
+ * Calls on one context must not run concurrently from several host threads. */
+int mgs_ctx_create(int device, size_t arena_bytes, mgs_ctx** out);
+int mgs_ctx_destroy(mgs_ctx* ctx);
+int mgs_ctx_synchronize(mgs_ctx* ctx); /* waits for the context's streams; reports device status words */
+int mgs_ctx_arena_bytes(mgs_ctx* ctx, size_t* bytes);
+
+/* Profiling: when enabled, every kernel launch of the context is bracketed by
+ * CUDA events on its stream. mgs_ctx_kernel_times synchronizes and returns, per
+ * kernel name, the number of launches and the summed device time; it then
+ * clears the record. */
+typedef struct mgs_kernel_time {
+  char name[48];
+  uint64_t launches;
+  double total_ms;
+} mgs_kernel_time;
+int mgs_ctx_set_profiling(mgs_ctx* ctx, int enabled);
+int mgs_ctx_kernel_times(mgs_ctx* ctx, mgs_kernel_time* out, int capacity, int* count);
+/* Number of kernels the context launched since the counter was last reset. */
+int mgs_ctx_launch_count(mgs_ctx* ctx, uint64_t* launches, int reset);
+
+/* ---- pinned host memory (HostVector<T>, src/host_vector.cuh:7) ---------- */
+int mgs_host_alloc(size_t bytes, void** out);
+int mgs_host_free(void* ptr);
+
+/* ---- device radix sort (thrust::sort on one GPU, src/tanasic_sort.cuh:264) ----
+ * Ascending, stable, in place on d_keys. d_temp must hold mgs_sort_temp_bytes()
+ * bytes, or be NULL to use the context arena. stream is a cudaStream_t (NULL =
+ * the context's compute stream). Asynchronous: device status is reported by
+ * mgs_ctx_synchronize. n must be below 2^32. */
+int mgs_sort_temp_bytes(int dtype, size_t n, size_t* bytes);
+int mgs_sort_device(mgs_ctx* ctx, int dtype, void* d_keys, size_t n, void* d_temp, size_t temp_bytes,
+                    void* stream);
+
+/* ---- TanasicSort with one GPU (src/tanasic_sort.cuh:223-299) ------------
+ * h_keys is the caller's host buffer (pinned for full link speed); sorted in
+ * place: H2D, device sort, D2H, synchronous. Returns early on n == 0 like the
+ * reference (src/tanasic_sort.cuh:225-227). */
+int mgs_sort_host(mgs_ctx* ctx, int dtype, void* h_keys, size_t n);
+
+/* ---- DataGenerator::ComputeDistribution<T> (src/data_generator.cuh:18-36) ----
+ * Fills the host buffer out[0..n) exactly as the reference generator does for
+ * the reference's distributions: "uniform", "normal", "zero", "staggered",
+ * "sorted", "reverse-sorted", "nearly-sorted", "bucket-sorted" (128 OpenMP
+ * threads, mt19937 per thread). Additional seeded distributions of the sort
+ * engine's workload sweep: "full-uniform", "normal0", "zipf", "sorted-full",
+ * "reverse-sorted-full", "nearly-sorted-swaps", "all-equal". For f32/f64 the
+ * "-specials" suffix (e.g. "full-uniform-specials") additionally replaces 0.1%
+ * of the keys with -0.0 and 0.1% with NaNs of both signs. */
+int mgs_generate(int dtype, const char* distribution, uint32_t seed, void* out, size_t n);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+#endif /* MGS_H_ */

@@ -1,0 +1,291 @@
+// C ABI of the sort engine (include/mgs.h). Argument checking, error strings,
+// context lifetime and the synchronous host-buffer entry points live here; the
+// device work is in csrc/kernels.
+#include "mgs.h"
+
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "../kernels/engine_types.h"
+#include "../kernels/radix_sort.cuh"
+#include "context.h"
+
+namespace mgs {
+bool generate_keys(int dtype, const char* distribution, uint32_t seed, void* out, size_t n);
+}
+
+using mgs::Context;
+using mgs::set_last_error;
+
+namespace {
+
+constexpr size_t kMaxDeviceSortKeys = (size_t(1) << 32) - 1;
+
+int cuda_fail(cudaError_t e, const char* what) {
+  set_last_error("%s: %s", what, cudaGetErrorString(e));
+  cudaGetLastError();  // clear the sticky-free error state
+  return e == cudaErrorMemoryAllocation ? MGS_ERR_OOM : MGS_ERR_CUDA;
+}
+
+int invalid(const char* msg) {
+  set_last_error("%s", msg);
+  return MGS_ERR_INVALID;
+}
+
+int status_to_code(uint32_t status) {
+  if (status == 0) return MGS_OK;
+  set_last_error("device status 0x%x: a bounded device-side wait gave up (%s%s%s)", status,
+                 (status & mgs::kStatusLookbackTimeout) ? "look-back " : "",
+                 (status & mgs::kStatusTmaTimeout) ? "tma " : "", (status & mgs::kStatusQueueTimeout) ? "queue " : "");
+  return MGS_ERR_TIMEOUT;
+}
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+inline size_t align256(size_t x) { return (x + 255) / 256 * 256; }
+
+}  // namespace
+
+extern "C" {
+
+int mgs_version(void) { return 10000 * 0 + 100 * 1 + 0; }
+
+const char* mgs_last_error_string(void) { return mgs::last_error(); }
+
+size_t mgs_dtype_size(int dtype) { return mgs::dtype_bytes(dtype); }
+
+int mgs_device_count(int* count) {
+  if (!count) return invalid("mgs_device_count: count is null");
+  int c = 0;
+  cudaError_t e = cudaGetDeviceCount(&c);
+  if (e != cudaSuccess) {
+    *count = 0;
+    cudaGetLastError();
+    set_last_error("cudaGetDeviceCount: %s", cudaGetErrorString(e));
+    return MGS_ERR_NO_DEVICE;
+  }
+  *count = c;
+  mgs::clear_last_error();
+  return MGS_OK;
+}
+
+int mgs_ctx_create(int device, size_t arena_bytes, mgs_ctx** out) {
+  if (!out) return invalid("mgs_ctx_create: out is null");
+  *out = nullptr;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+    cudaGetLastError();
+    set_last_error("mgs_ctx_create: no CUDA device");
+    return MGS_ERR_NO_DEVICE;
+  }
+  if (device < 0 || device >= count) {
+    set_last_error("mgs_ctx_create: device %d out of range [0, %d)", device, count);
+    return MGS_ERR_NO_DEVICE;
+  }
+  DeviceGuard g(device);
+  mgs_ctx* ctx = new (std::nothrow) mgs_ctx();
+  if (!ctx) return invalid("mgs_ctx_create: out of host memory");
+  Context& c = ctx->impl;
+  c.device = device;
+  cudaDeviceGetAttribute(&c.sm_count, cudaDevAttrMultiProcessorCount, device);
+  cudaError_t e = cudaStreamCreateWithFlags(&c.compute, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c.h2d, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c.d2h, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaMalloc(&c.d_status, 256);
+  if (e == cudaSuccess) e = cudaMemset(c.d_status, 0, 256);
+  if (e == cudaSuccess) e = cudaMallocHost(&c.h_status, 256);
+  if (e == cudaSuccess && arena_bytes > 0) e = c.reserve(arena_bytes);
+  if (e != cudaSuccess) {
+    int rc = cuda_fail(e, "mgs_ctx_create");
+    mgs_ctx_destroy(ctx);
+    return rc;
+  }
+  *out = ctx;
+  mgs::clear_last_error();
+  return MGS_OK;
+}
+
+int mgs_ctx_destroy(mgs_ctx* ctx) {
+  if (!ctx) return MGS_OK;
+  Context& c = ctx->impl;
+  {
+    DeviceGuard g(c.device);
+    if (c.compute) cudaStreamSynchronize(c.compute);
+    if (c.h2d) cudaStreamSynchronize(c.h2d);
+    if (c.d2h) cudaStreamSynchronize(c.d2h);
+    if (c.arena) cudaFree(c.arena);
+    if (c.d_status) cudaFree(c.d_status);
+    if (c.h_status) cudaFreeHost(c.h_status);
+    if (c.compute) cudaStreamDestroy(c.compute);
+    if (c.h2d) cudaStreamDestroy(c.h2d);
+    if (c.d2h) cudaStreamDestroy(c.d2h);
+    delete ctx;
+  }
+  mgs::clear_last_error();
+  return MGS_OK;
+}
+
+int mgs_ctx_synchronize(mgs_ctx* ctx) {
+  if (!ctx) return invalid("mgs_ctx_synchronize: ctx is null");
+  Context& c = ctx->impl;
+  DeviceGuard g(c.device);
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) return cuda_fail(e, "mgs_ctx_synchronize");
+  uint32_t status = 0;
+  e = c.take_status(c.compute, &status);
+  if (e != cudaSuccess) return cuda_fail(e, "mgs_ctx_synchronize: status read");
+  int rc = status_to_code(status);
+  if (rc == MGS_OK) mgs::clear_last_error();
+  return rc;
+}
+
+int mgs_ctx_arena_bytes(mgs_ctx* ctx, size_t* bytes) {
+  if (!ctx || !bytes) return invalid("mgs_ctx_arena_bytes: null argument");
+  *bytes = ctx->impl.arena_bytes;
+  return MGS_OK;
+}
+
+int mgs_ctx_set_profiling(mgs_ctx* ctx, int enabled) {
+  if (!ctx) return invalid("mgs_ctx_set_profiling: ctx is null");
+  ctx->impl.recorder.set_enabled(enabled != 0);
+  return MGS_OK;
+}
+
+int mgs_ctx_kernel_times(mgs_ctx* ctx, mgs_kernel_time* out, int capacity, int* count) {
+  if (!ctx || !count || (capacity > 0 && !out)) return invalid("mgs_ctx_kernel_times: null argument");
+  DeviceGuard g(ctx->impl.device);
+  std::vector<std::pair<std::string, std::pair<uint64_t, double>>> rows;
+  cudaError_t e = ctx->impl.recorder.collect(&rows);
+  if (e != cudaSuccess) return cuda_fail(e, "mgs_ctx_kernel_times");
+  *count = int(rows.size());
+  for (int i = 0; i < capacity && i < int(rows.size()); ++i) {
+    std::memset(out[i].name, 0, sizeof(out[i].name));
+    std::strncpy(out[i].name, rows[i].first.c_str(), sizeof(out[i].name) - 1);
+    out[i].launches = rows[i].second.first;
+    out[i].total_ms = rows[i].second.second;
+  }
+  return MGS_OK;
+}
+
+int mgs_ctx_launch_count(mgs_ctx* ctx, uint64_t* launches, int reset) {
+  if (!ctx || !launches) return invalid("mgs_ctx_launch_count: null argument");
+  *launches = ctx->impl.recorder.launches();
+  if (reset) ctx->impl.recorder.reset_launches();
+  return MGS_OK;
+}
+
+int mgs_host_alloc(size_t bytes, void** out) {
+  if (!out) return invalid("mgs_host_alloc: out is null");
+  *out = nullptr;
+  if (bytes == 0) return MGS_OK;
+  cudaError_t e = cudaMallocHost(out, bytes);
+  if (e != cudaSuccess) {
+    *out = nullptr;
+    cudaGetLastError();
+    set_last_error("mgs_host_alloc(%zu): %s", bytes, cudaGetErrorString(e));
+    return MGS_ERR_OOM;
+  }
+  return MGS_OK;
+}
+
+int mgs_host_free(void* ptr) {
+  if (!ptr) return MGS_OK;
+  cudaError_t e = cudaFreeHost(ptr);
+  if (e != cudaSuccess) return cuda_fail(e, "mgs_host_free");
+  return MGS_OK;
+}
+
+int mgs_sort_temp_bytes(int dtype, size_t n, size_t* bytes) {
+  if (!bytes) return invalid("mgs_sort_temp_bytes: bytes is null");
+  if (mgs::dtype_bytes(dtype) == 0) return invalid("mgs_sort_temp_bytes: unknown dtype");
+  if (n > kMaxDeviceSortKeys) return invalid("mgs_sort_temp_bytes: n must be below 2^32");
+  *bytes = mgs::radix_sort_temp_bytes(dtype, n);
+  return MGS_OK;
+}
+
+int mgs_sort_device(mgs_ctx* ctx, int dtype, void* d_keys, size_t n, void* d_temp, size_t temp_bytes,
+                    void* stream) {
+  if (!ctx) return invalid("mgs_sort_device: ctx is null");
+  const size_t w = mgs::dtype_bytes(dtype);
+  if (w == 0) return invalid("mgs_sort_device: unknown dtype");
+  if (n == 0) return MGS_OK;
+  if (!d_keys) return invalid("mgs_sort_device: d_keys is null");
+  if (reinterpret_cast<uintptr_t>(d_keys) % w != 0) return invalid("mgs_sort_device: d_keys is not key-aligned");
+  if (n > kMaxDeviceSortKeys) return invalid("mgs_sort_device: n must be below 2^32 (use the chunked entry points)");
+  Context& c = ctx->impl;
+  DeviceGuard g(c.device);
+  const size_t need = mgs::radix_sort_temp_bytes(dtype, n);
+  if (d_temp == nullptr) {
+    cudaError_t e = c.reserve(need);
+    if (e != cudaSuccess) return cuda_fail(e, "mgs_sort_device: arena");
+    d_temp = c.arena;
+    temp_bytes = c.arena_bytes;
+  } else if (temp_bytes < need) {
+    set_last_error("mgs_sort_device: d_temp holds %zu bytes, %zu needed", temp_bytes, need);
+    return MGS_ERR_INVALID;
+  }
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c.compute;
+  cudaError_t e = mgs::radix_sort(dtype, d_keys, n, d_temp, temp_bytes, s, c.d_status, &c.recorder);
+  if (e != cudaSuccess) return cuda_fail(e, "mgs_sort_device");
+  mgs::clear_last_error();
+  return MGS_OK;
+}
+
+int mgs_sort_host(mgs_ctx* ctx, int dtype, void* h_keys, size_t n) {
+  if (!ctx) return invalid("mgs_sort_host: ctx is null");
+  const size_t w = mgs::dtype_bytes(dtype);
+  if (w == 0) return invalid("mgs_sort_host: unknown dtype");
+  if (n == 0) return MGS_OK;  // src/tanasic_sort.cuh:225-227
+  if (!h_keys) return invalid("mgs_sort_host: h_keys is null");
+  if (n > kMaxDeviceSortKeys) return invalid("mgs_sort_host: n must be below 2^32");
+  Context& c = ctx->impl;
+  DeviceGuard g(c.device);
+  const size_t bytes = n * w;
+  const size_t keys_bytes = align256(bytes);
+  const size_t temp = mgs::radix_sort_temp_bytes(dtype, n);
+  cudaError_t e = c.reserve(keys_bytes + temp);
+  if (e != cudaSuccess) return cuda_fail(e, "mgs_sort_host: arena");
+  char* base = static_cast<char*>(c.arena);
+  void* d_keys = base;
+  void* d_temp = base + keys_bytes;
+  e = cudaMemcpyAsync(d_keys, h_keys, bytes, cudaMemcpyHostToDevice, c.compute);
+  if (e != cudaSuccess) return cuda_fail(e, "mgs_sort_host: H2D");
+  e = mgs::radix_sort(dtype, d_keys, n, d_temp, c.arena_bytes - keys_bytes, c.compute, c.d_status, &c.recorder);
+  if (e != cudaSuccess) return cuda_fail(e, "mgs_sort_host: sort");
+  e = cudaMemcpyAsync(h_keys, d_keys, bytes, cudaMemcpyDeviceToHost, c.compute);
+  if (e != cudaSuccess) return cuda_fail(e, "mgs_sort_host: D2H");
+  uint32_t status = 0;
+  e = c.take_status(c.compute, &status);
+  if (e != cudaSuccess) return cuda_fail(e, "mgs_sort_host: synchronize");
+  int rc = status_to_code(status);
+  if (rc == MGS_OK) mgs::clear_last_error();
+  return rc;
+}
+
+int mgs_generate(int dtype, const char* distribution, uint32_t seed, void* out, size_t n) {
+  if (!distribution) return invalid("mgs_generate: distribution is null");
+  if (mgs::dtype_bytes(dtype) == 0) return invalid("mgs_generate: unknown dtype");
+  if (n == 0) return MGS_OK;
+  if (!out) return invalid("mgs_generate: out is null");
+  if (!mgs::generate_keys(dtype, distribution, seed, out, n)) {
+    set_last_error("mgs_generate: unknown distribution '%s' for this dtype", distribution);
+    return MGS_ERR_INVALID;
+  }
+  mgs::clear_last_error();
+  return MGS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,518 @@
+// Onesweep LSD radix sort for one B200 (sm_100a): the engine's replacement of
+// thrust::sort -> CUB DeviceRadixSort, which the reference calls for every
+// partition / chunk sort (src/tanasic_sort.cuh:264-266,
+// src/gowanlock_sort.cuh:188-190,337-339, src/sort_benchmark.cu:300).
+//
+// Per sort of n keys of w bytes (P = w 8-bit digit passes):
+//   K1 radix_histogram : one streaming read of the keys builds all P digit
+//                        histograms at once (16-byte loads, shared-memory
+//                        sub-histograms) and clears the first look-back array.
+//   K1b radix_scan     : exclusive scan per pass -> global bucket starts; marks
+//                        passes whose digit is the same for every key (the
+//                        stable counting pass is then the identity and is skipped).
+//   K2 radix_onesweep  : one launch per pass. Each CTA takes the next tile in
+//                        launch order from an atomic counter, stages it in shared
+//                        memory with a TMA bulk copy, ranks the keys by digit with
+//                        warp match (or ballots) and shared-memory counters,
+//                        publishes its digit counts, resolves its global offsets
+//                        by decoupled look-back over earlier tiles, and scatters
+//                        the tile from shared memory in digit order.
+//   K3 radix_finalize  : when an odd number of passes ran, copies the result back
+//                        into the caller's buffer; reports device status words.
+// Algorithmic HBM traffic: n*w*(2P+1) bytes (+ n*w*2 for an odd pass count).
+#include <algorithm>
+#include <mutex>
+
+#include "device_common.cuh"
+#include "dispatch.cuh"
+#include "radix_sort.cuh"
+
+namespace mgs {
+namespace {
+
+constexpr int kRadix = 256;
+constexpr int kMaxPasses = 8;
+
+struct RadixState {
+  uint32_t counts[kMaxPasses][kRadix];        // global digit counts (atomically accumulated)
+  uint32_t bucket_start[kMaxPasses][kRadix];  // exclusive scan of counts
+  uint32_t tile_counter[kMaxPasses];          // launch-order tile ids per pass
+  uint32_t skip[kMaxPasses];                  // 1 = every key has the same digit in this pass
+  uint32_t error;                             // DeviceStatus bits
+  uint32_t pad[7];
+};
+
+// Tile shape per key width (threads x keys per thread).
+template <int KEY_BYTES>
+struct OnesweepShape;
+template <>
+struct OnesweepShape<4> {
+  static constexpr int kBlock = 256;
+  static constexpr int kItems = 16;
+};
+template <>
+struct OnesweepShape<8> {
+  static constexpr int kBlock = 256;
+  static constexpr int kItems = 8;
+};
+
+constexpr int kHistBlock = 256;
+constexpr int kHistSub = 4;
+constexpr int kHistUnroll = 4;
+constexpr uint32_t kLookbackSpinLimit = 1u << 25;
+constexpr uint32_t kTmaWaitLimit = 1u << 24;
+
+// Look-back status word: 0 = not published yet; (count + 1) with the top bit
+// clear = this tile's own digit count (aggregate); top bit set = inclusive
+// prefix over this tile and all earlier ones.
+template <typename StatusT>
+struct LookbackWord;
+template <>
+struct LookbackWord<uint32_t> {
+  static constexpr uint32_t kPrefix = 0x80000000u;
+  __device__ __forceinline__ static uint32_t load(const uint32_t* p) { return ld_volatile_u32(p); }
+  __device__ __forceinline__ static void store(uint32_t* p, uint32_t v) { st_volatile_u32(p, v); }
+};
+template <>
+struct LookbackWord<unsigned long long> {
+  static constexpr unsigned long long kPrefix = 0x8000000000000000ull;
+  __device__ __forceinline__ static unsigned long long load(const unsigned long long* p) {
+    return ld_volatile_u64(p);
+  }
+  __device__ __forceinline__ static void store(unsigned long long* p, unsigned long long v) {
+    st_volatile_u64(p, v);
+  }
+};
+
+template <typename Bits>
+__device__ __forceinline__ void unpack_v4(const uint4& q, Bits (&k)[16 / sizeof(Bits)]);
+template <>
+__device__ __forceinline__ void unpack_v4<uint32_t>(const uint4& q, uint32_t (&k)[4]) {
+  k[0] = q.x;
+  k[1] = q.y;
+  k[2] = q.z;
+  k[3] = q.w;
+}
+template <>
+__device__ __forceinline__ void unpack_v4<unsigned long long>(const uint4& q, unsigned long long (&k)[2]) {
+  k[0] = (static_cast<unsigned long long>(q.y) << 32) | q.x;
+  k[1] = (static_cast<unsigned long long>(q.w) << 32) | q.z;
+}
+
+// ---------------------------------------------------------------- K1 --------
+template <class Tr>
+__global__ __launch_bounds__(kHistBlock) void radix_histogram_kernel(const typename Tr::Bits* __restrict__ keys,
+                                                                     uint32_t n, RadixState* __restrict__ st,
+                                                                     uint4* __restrict__ lb0, size_t lb0_vecs) {
+  using Bits = typename Tr::Bits;
+  constexpr int P = Tr::kPasses;
+  constexpr int kPerVec = 16 / int(sizeof(Bits));
+  __shared__ uint32_t sh[kHistSub][P][kRadix];
+  uint32_t* shf = &sh[0][0][0];
+  for (int i = threadIdx.x; i < kHistSub * P * kRadix; i += kHistBlock) shf[i] = 0u;
+
+  const size_t gtid = size_t(blockIdx.x) * kHistBlock + threadIdx.x;
+  const size_t gstride = size_t(gridDim.x) * kHistBlock;
+  for (size_t i = gtid; i < lb0_vecs; i += gstride) lb0[i] = make_uint4(0u, 0u, 0u, 0u);
+  __syncthreads();
+
+  uint32_t(*hs)[kRadix] = sh[(threadIdx.x >> 5) % kHistSub];
+  auto count_key = [&](Bits k) {
+    const Bits o = Tr::Ordered(k);
+#pragma unroll
+    for (int p = 0; p < P; ++p) atomicAdd(&hs[p][uint32_t(o >> (8 * p)) & 0xFFu], 1u);
+  };
+
+  const uintptr_t addr = reinterpret_cast<uintptr_t>(keys);
+  size_t head = ((16u - (addr & 15u)) & 15u) / sizeof(Bits);
+  if (head > n) head = n;
+  const size_t nvec = (n - head) / kPerVec;
+  const uint4* kv = reinterpret_cast<const uint4*>(keys + head);
+  if (blockIdx.x == 0) {
+    for (size_t i = threadIdx.x; i < head; i += kHistBlock) count_key(keys[i]);
+    for (size_t i = head + nvec * kPerVec + threadIdx.x; i < n; i += kHistBlock) count_key(keys[i]);
+  }
+  size_t v = gtid;
+  for (; v + (kHistUnroll - 1) * gstride < nvec; v += kHistUnroll * gstride) {
+    uint4 q[kHistUnroll];
+#pragma unroll
+    for (int u = 0; u < kHistUnroll; ++u) q[u] = ld_stream_v4(kv + v + u * gstride);
+#pragma unroll
+    for (int u = 0; u < kHistUnroll; ++u) {
+      Bits k[kPerVec];
+      unpack_v4<Bits>(q[u], k);
+#pragma unroll
+      for (int j = 0; j < kPerVec; ++j) count_key(k[j]);
+    }
+  }
+  for (; v < nvec; v += gstride) {
+    Bits k[kPerVec];
+    unpack_v4<Bits>(ld_stream_v4(kv + v), k);
+#pragma unroll
+    for (int j = 0; j < kPerVec; ++j) count_key(k[j]);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < P * kRadix; i += kHistBlock) {
+    uint32_t s = 0;
+#pragma unroll
+    for (int sub = 0; sub < kHistSub; ++sub) s += shf[sub * P * kRadix + i];
+    if (s) atomicAdd(&st->counts[i / kRadix][i % kRadix], s);
+  }
+}
+
+// ---------------------------------------------------------------- K1b -------
+__global__ __launch_bounds__(kRadix) void radix_scan_kernel(RadixState* __restrict__ st, uint32_t n) {
+  __shared__ uint32_t tmp[kRadix / 32 + 1];
+  const int p = blockIdx.x, d = threadIdx.x;
+  const uint32_t c = st->counts[p][d];
+  if (c == n) st->skip[p] = 1u;
+  uint32_t total;
+  const uint32_t ex = block_exclusive_scan<kRadix>(c, tmp, &total);
+  st->bucket_start[p][d] = ex;
+}
+
+// ---------------------------------------------------------------- K2 --------
+template <class Tr, int BLOCK, int ITEMS>
+struct OnesweepSmem {
+  static constexpr int kTile = BLOCK * ITEMS;
+  static constexpr int kWarps = BLOCK / 32;
+  typename Tr::Bits keys[kTile];  // staged tile, then the tile in digit order
+  uint32_t whist[kWarps * kRadix];  // per-warp digit counters -> per-warp offsets
+  uint32_t tile_start[kRadix];      // exclusive scan of the tile's digit counts
+  uint32_t gbase[kRadix];           // global scatter base per digit
+  uint32_t scan_tmp[kWarps + 1];
+  uint32_t tile_id;
+  alignas(8) uint64_t bar;
+};
+
+// Peer mask of lanes holding the same digit. MATCH=0 uses match.any, MATCH=1
+// builds it from 8 ballots (one per digit bit); `ok` separates padding lanes.
+template <int MATCH, bool FULL>
+__device__ __forceinline__ uint32_t digit_peers(uint32_t d, bool ok) {
+  if (MATCH == 0) {
+    return __match_any_sync(0xffffffffu, d);
+  } else {
+    uint32_t peers = 0xffffffffu;
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+      const bool bit = (d >> b) & 1u;
+      const uint32_t bal = __ballot_sync(0xffffffffu, bit);
+      peers &= bit ? bal : ~bal;
+    }
+    if (!FULL) {
+      const uint32_t bal = __ballot_sync(0xffffffffu, ok);
+      peers &= ok ? bal : ~bal;
+    }
+    return peers;
+  }
+}
+
+template <class Tr, int BLOCK, int ITEMS, typename StatusT, int MATCH, bool FULL>
+__device__ __forceinline__ void onesweep_tile(OnesweepSmem<Tr, BLOCK, ITEMS>& sm, RadixState* __restrict__ st,
+                                              StatusT* __restrict__ lb_cur, typename Tr::Bits* __restrict__ dst,
+                                              uint32_t tile, uint32_t valid, uint32_t n, int pass) {
+  using Bits = typename Tr::Bits;
+  using LW = LookbackWord<StatusT>;
+  constexpr int kTile = BLOCK * ITEMS;
+  constexpr int kWarps = BLOCK / 32;
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5, lane = tid & 31;
+  uint32_t* wh = sm.whist + warp * kRadix;
+  const uint32_t lmask = lanemask_lt();
+
+  // Rank each key among the keys of its warp with the same digit. Warp w owns
+  // tile positions [w*32*ITEMS, (w+1)*32*ITEMS), item i of lane l is position
+  // w*32*ITEMS + i*32 + l, so ranks follow input order (stability).
+  Bits key[ITEMS];
+  uint32_t rank[ITEMS];
+  const int wbase = warp * 32 * ITEMS;
+#pragma unroll
+  for (int i = 0; i < ITEMS; ++i) {
+    const uint32_t idx = wbase + i * 32 + lane;
+    const bool ok = FULL || idx < valid;
+    key[i] = sm.keys[idx];
+    const uint32_t d = ok ? Tr::Digit(key[i], pass) : (256u + lane);
+    const uint32_t peers = digit_peers<MATCH, FULL>(d, ok);
+    const uint32_t before = __popc(peers & lmask);
+    const uint32_t cnt = ok ? wh[d] : 0u;
+    __syncwarp();
+    if (ok && before == 0) wh[d] = cnt + __popc(peers);
+    __syncwarp();
+    rank[i] = cnt + before;
+  }
+  __syncthreads();
+
+  // Per digit: turn the warp counters into exclusive per-warp offsets, publish
+  // the tile's count for the look-back, and scan the counts across digits.
+  uint32_t tile_count = 0;
+  if (tid < kRadix) {
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) {
+      const uint32_t t = sm.whist[w * kRadix + tid];
+      sm.whist[w * kRadix + tid] = tile_count;
+      tile_count += t;
+    }
+    StatusT* slot = lb_cur + size_t(tile) * kRadix + tid;
+    LW::store(slot, tile == 0 ? (LW::kPrefix | StatusT(tile_count)) : StatusT(tile_count + 1u));
+  }
+  uint32_t total;
+  const uint32_t tstart = block_exclusive_scan<BLOCK>(tid < kRadix ? tile_count : 0u, sm.scan_tmp, &total);
+  if (tid < kRadix) sm.tile_start[tid] = tstart;
+  __syncthreads();
+
+  // Stage the tile in digit order in shared memory.
+#pragma unroll
+  for (int i = 0; i < ITEMS; ++i) {
+    const uint32_t idx = wbase + i * 32 + lane;
+    if (FULL || idx < valid) {
+      const uint32_t d = Tr::Digit(key[i], pass);
+      const uint32_t pos = sm.tile_start[d] + wh[d] + rank[i];
+      if (pos < uint32_t(kTile)) sm.keys[pos] = key[i];
+    }
+  }
+
+  // Decoupled look-back: one thread per digit walks back over earlier tiles,
+  // summing their aggregates until it meets an inclusive prefix.
+  if (tid < kRadix) {
+    StatusT excl = 0;
+    if (tile > 0) {
+      long long j = static_cast<long long>(tile) - 1;
+      uint32_t spins = 0;
+      while (j >= 0) {
+        const StatusT s = LW::load(lb_cur + size_t(j) * kRadix + tid);
+        if (s == 0) {
+          if (++spins >= kLookbackSpinLimit) {
+            atomicOr(&st->error, kStatusLookbackTimeout);
+            break;
+          }
+          if (spins > 16) __nanosleep(32);
+          continue;
+        }
+        if (s & LW::kPrefix) {
+          excl += s & ~LW::kPrefix;
+          break;
+        }
+        excl += s - 1;
+        --j;
+      }
+      LW::store(lb_cur + size_t(tile) * kRadix + tid, LW::kPrefix | (excl + tile_count));
+    }
+    sm.gbase[tid] = st->bucket_start[pass][tid] + uint32_t(excl) - sm.tile_start[tid];
+  }
+  __syncthreads();
+
+  // Scatter: consecutive threads write consecutive positions of one digit run.
+  // The bound check only fails after a look-back timeout (status already set).
+#pragma unroll
+  for (int i = 0; i < ITEMS; ++i) {
+    const uint32_t idx = i * BLOCK + tid;
+    if (FULL || idx < valid) {
+      const Bits k = sm.keys[idx];
+      const uint32_t d = Tr::Digit(k, pass);
+      const uint32_t pos = sm.gbase[d] + idx;
+      if (pos < n) dst[pos] = k;
+    }
+  }
+}
+
+template <class Tr, int BLOCK, int ITEMS, typename StatusT, int MATCH>
+__global__ __launch_bounds__(BLOCK) void radix_onesweep_kernel(typename Tr::Bits* buf0, typename Tr::Bits* buf1,
+                                                               RadixState* __restrict__ st,
+                                                               StatusT* __restrict__ lb_cur,
+                                                               StatusT* __restrict__ lb_next, uint32_t n, int pass,
+                                                               int use_tma) {
+  using Bits = typename Tr::Bits;
+  using Smem = OnesweepSmem<Tr, BLOCK, ITEMS>;
+  constexpr int kTile = Smem::kTile;
+  constexpr int kWarps = Smem::kWarps;
+  static_assert(BLOCK >= kRadix, "one thread per digit");
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  Smem& sm = *reinterpret_cast<Smem*>(smem_raw);
+  const int tid = threadIdx.x;
+
+  // The next pass uses the other look-back array; this CTA clears its slots.
+  if (lb_next != nullptr && tid < kRadix) lb_next[size_t(blockIdx.x) * kRadix + tid] = 0;
+
+  if (st->skip[pass]) return;  // one digit for every key: identity permutation
+  int sel = 0;
+  for (int q = 0; q < pass; ++q) sel ^= (st->skip[q] == 0u) ? 1 : 0;
+  const Bits* src = sel ? buf1 : buf0;
+  Bits* dst = sel ? buf0 : buf1;
+
+  if (tid == 0) {
+    const uint32_t t = atomicAdd(&st->tile_counter[pass], 1u);
+    sm.tile_id = t;
+    const size_t base = size_t(t) * kTile;
+    if (use_tma && base + kTile <= n) {
+      mbar_init(&sm.bar, 1);
+      fence_mbar_init();
+      mbar_arrive_expect_tx(&sm.bar, uint32_t(kTile * sizeof(Bits)));
+      bulk_copy_g2s(sm.keys, src + base, uint32_t(kTile * sizeof(Bits)), &sm.bar);
+    }
+  }
+  for (int i = tid; i < kWarps * kRadix; i += BLOCK) sm.whist[i] = 0u;
+  __syncthreads();
+  const uint32_t tile = sm.tile_id;
+  const size_t base = size_t(tile) * kTile;
+  const uint32_t valid = uint32_t(min(size_t(kTile), size_t(n) - base));
+  if (use_tma && valid == uint32_t(kTile)) {
+    const bool arrived = mbar_wait_bounded(&sm.bar, 0, kTmaWaitLimit);
+    if (__syncthreads_or(!arrived)) {  // block-uniform exit when the copy never completed
+      if (tid == 0) atomicOr(&st->error, kStatusTmaTimeout);
+      return;
+    }
+  } else {
+    for (uint32_t i = tid; i < valid; i += BLOCK) sm.keys[i] = src[base + i];
+    __syncthreads();
+  }
+  if (valid == uint32_t(kTile)) {
+    onesweep_tile<Tr, BLOCK, ITEMS, StatusT, MATCH, true>(sm, st, lb_cur, dst, tile, valid, n, pass);
+  } else {
+    onesweep_tile<Tr, BLOCK, ITEMS, StatusT, MATCH, false>(sm, st, lb_cur, dst, tile, valid, n, pass);
+  }
+}
+
+// ---------------------------------------------------------------- K3 --------
+template <class Tr>
+__global__ __launch_bounds__(256) void radix_finalize_kernel(typename Tr::Bits* __restrict__ buf0,
+                                                             const typename Tr::Bits* __restrict__ buf1,
+                                                             const RadixState* __restrict__ st, uint32_t n,
+                                                             uint32_t* __restrict__ d_status) {
+  using Bits = typename Tr::Bits;
+  int live = 0;
+#pragma unroll
+  for (int p = 0; p < Tr::kPasses; ++p) live += (st->skip[p] == 0u) ? 1 : 0;
+  if (blockIdx.x == 0 && threadIdx.x == 0 && d_status != nullptr && st->error != 0u) atomicOr(d_status, st->error);
+  if ((live & 1) == 0) return;
+  const size_t gtid = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  const size_t gstride = size_t(gridDim.x) * blockDim.x;
+  const bool aligned = ((reinterpret_cast<uintptr_t>(buf0) | reinterpret_cast<uintptr_t>(buf1)) & 15u) == 0;
+  if (aligned) {
+    constexpr int kPerVec = 16 / int(sizeof(Bits));
+    const size_t nvec = n / kPerVec;
+    const uint4* s = reinterpret_cast<const uint4*>(buf1);
+    uint4* d = reinterpret_cast<uint4*>(buf0);
+    for (size_t i = gtid; i < nvec; i += gstride) d[i] = ld_stream_v4(s + i);
+    for (size_t i = nvec * kPerVec + gtid; i < n; i += gstride) buf0[i] = buf1[i];
+  } else {
+    for (size_t i = gtid; i < n; i += gstride) buf0[i] = buf1[i];
+  }
+}
+
+// ---------------------------------------------------------------- host ------
+size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+struct RadixLayout {
+  size_t state_off, lb0_off, lb1_off, keys_off, total;
+  size_t num_tiles, status_bytes;
+};
+
+template <class Tr>
+RadixLayout radix_layout(size_t n) {
+  using Shape = OnesweepShape<sizeof(typename Tr::Bits)>;
+  constexpr size_t kTile = size_t(Shape::kBlock) * Shape::kItems;
+  RadixLayout L;
+  L.num_tiles = (n + kTile - 1) / kTile;
+  L.status_bytes = (n < (size_t(1) << 31)) ? 4 : 8;
+  const size_t lb_bytes = L.num_tiles * kRadix * L.status_bytes;
+  L.state_off = 0;
+  L.lb0_off = align_up(sizeof(RadixState), 256);
+  L.lb1_off = L.lb0_off + align_up(lb_bytes, 256);
+  L.keys_off = L.lb1_off + align_up(lb_bytes, 256);
+  L.total = L.keys_off + align_up(n * sizeof(typename Tr::Bits), 256);
+  return L;
+}
+
+int device_sm_count() {
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return sms > 0 ? sms : 148;
+}
+
+template <class Tr, typename StatusT, int MATCH>
+cudaError_t launch_onesweep_passes(typename Tr::Bits* keys, typename Tr::Bits* tmp, RadixState* st, char* tbase,
+                                   const RadixLayout& L, uint32_t n, bool use_tma, cudaStream_t stream,
+                                   LaunchRecorder* rec) {
+  using Shape = OnesweepShape<sizeof(typename Tr::Bits)>;
+  using Smem = OnesweepSmem<Tr, Shape::kBlock, Shape::kItems>;
+  auto kernel = radix_onesweep_kernel<Tr, Shape::kBlock, Shape::kItems, StatusT, MATCH>;
+  static std::once_flag once;
+  std::call_once(once, [&] {
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(Smem)));
+  });
+  StatusT* lb[2] = {reinterpret_cast<StatusT*>(tbase + L.lb0_off), reinterpret_cast<StatusT*>(tbase + L.lb1_off)};
+  for (int p = 0; p < Tr::kPasses; ++p) {
+    StatusT* cur = lb[p & 1];
+    StatusT* next = (p + 1 < Tr::kPasses) ? lb[(p + 1) & 1] : nullptr;
+    cudaError_t e = launch_kernel(rec, "radix_onesweep", kernel, dim3(unsigned(L.num_tiles)), dim3(Shape::kBlock),
+                                  sizeof(Smem), stream, keys, tmp, st, cur, next, n, p, use_tma ? 1 : 0);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+template <class Tr>
+cudaError_t radix_sort_typed(typename Tr::Bits* keys, size_t n, void* temp, size_t temp_bytes, cudaStream_t stream,
+                             uint32_t* d_status, LaunchRecorder* rec) {
+  using Bits = typename Tr::Bits;
+  if (n == 0) return cudaSuccess;
+  if (n >= (size_t(1) << 32)) return cudaErrorInvalidValue;
+  const RadixLayout L = radix_layout<Tr>(n);
+  if (temp == nullptr || temp_bytes < L.total) return cudaErrorInvalidValue;
+  char* tb = static_cast<char*>(temp);
+  RadixState* st = reinterpret_cast<RadixState*>(tb + L.state_off);
+  Bits* tmp = reinterpret_cast<Bits*>(tb + L.keys_off);
+  const uint32_t n32 = uint32_t(n);
+  cudaError_t e = cudaMemsetAsync(st, 0, sizeof(RadixState), stream);
+  if (e != cudaSuccess) return e;
+
+  const int sms = device_sm_count();
+  const size_t vecs = n * sizeof(Bits) / 16 + 1;
+  const size_t want = (vecs + size_t(kHistBlock) * kHistUnroll - 1) / (size_t(kHistBlock) * kHistUnroll);
+  const unsigned hist_grid = unsigned(std::max<size_t>(1, std::min<size_t>(size_t(sms) * 4, want)));
+  const size_t lb0_vecs = L.num_tiles * kRadix * L.status_bytes / 16;
+  e = launch_kernel(rec, "radix_histogram", radix_histogram_kernel<Tr>, dim3(hist_grid), dim3(kHistBlock), 0,
+                    stream, keys, n32, st, reinterpret_cast<uint4*>(tb + L.lb0_off), lb0_vecs);
+  if (e != cudaSuccess) return e;
+  e = launch_kernel(rec, "radix_scan", radix_scan_kernel, dim3(Tr::kPasses), dim3(kRadix), 0, stream, st, n32);
+  if (e != cudaSuccess) return e;
+
+  const bool use_tma = (reinterpret_cast<uintptr_t>(keys) & 15u) == 0;
+  if (L.status_bytes == 4) {
+    e = launch_onesweep_passes<Tr, uint32_t, 0>(keys, tmp, st, tb, L, n32, use_tma, stream, rec);
+  } else {
+    e = launch_onesweep_passes<Tr, unsigned long long, 0>(keys, tmp, st, tb, L, n32, use_tma, stream, rec);
+  }
+  if (e != cudaSuccess) return e;
+
+  const unsigned fin_grid = unsigned(std::max<size_t>(1, std::min<size_t>(size_t(sms) * 8, (n + 1023) / 1024)));
+  return launch_kernel(rec, "radix_finalize", radix_finalize_kernel<Tr>, dim3(fin_grid), dim3(256), 0, stream, keys,
+                       tmp, st, n32, d_status);
+}
+
+}  // namespace
+
+size_t radix_sort_temp_bytes(int dtype, size_t n) {
+  size_t bytes = 0;
+  dispatch_dtype(dtype, [&](auto tr) { bytes = radix_layout<decltype(tr)>(n).total; });
+  return bytes;
+}
+
+int radix_sort_launches(int dtype, size_t n) {
+  if (n == 0) return 0;
+  const size_t w = dtype_bytes(dtype);
+  return int(3 + w);  // histogram + scan + one onesweep per 8-bit digit + finalize
+}
+
+cudaError_t radix_sort(int dtype, void* d_keys, size_t n, void* d_temp, size_t temp_bytes, cudaStream_t stream,
+                       uint32_t* d_status, LaunchRecorder* rec) {
+  cudaError_t result = cudaErrorInvalidValue;
+  dispatch_dtype(dtype, [&](auto tr) {
+    using Tr = decltype(tr);
+    result = radix_sort_typed<Tr>(static_cast<typename Tr::Bits*>(d_keys), n, d_temp, temp_bytes, stream, d_status,
+                                  rec);
+  });
+  return result;
+}
+
+}  // namespace mgs

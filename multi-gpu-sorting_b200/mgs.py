@@ -1,0 +1,220 @@
+"""Python binding of the sort engine's C ABI (include/mgs.h) over ctypes.
+
+The engine itself is native: lib/libmgs.so (CUDA kernels for sm_100a + C++
+host runtime). This module only marshals arguments. It never falls back to a
+CPU path: if the library or a GPU is missing, calls raise MgsError.
+
+Reference surface (hpides/multi-gpu-sorting) mirrored here:
+  TanasicSort<T>(HostVector<T>*, gpus)       -> tanasic_sort(array, gpus)
+  GowanlockSort<T>(HostVector<T>*, ...)      -> gowanlock_sort(array, ...)
+  DataGenerator(seed).ComputeDistribution<T> -> DataGenerator(seed).compute_distribution(...)
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import weakref
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libmgs.so")
+
+MGS_OK = 0
+MGS_ERR_INVALID = 1
+MGS_ERR_OOM = 2
+MGS_ERR_CUDA = 3
+MGS_ERR_TIMEOUT = 4
+MGS_ERR_NO_DEVICE = 5
+MGS_ERR_CANCELLED = 6
+MGS_ERR_BUSY = 7
+
+# mgs_dtype codes and their numpy storage types. The reference CLI names
+# int/long/float/double (src/sort_benchmark.cu:420-432).
+DTYPES = {
+    "u32": (0, np.uint32),
+    "i32": (1, np.int32),
+    "f32": (2, np.float32),
+    "u64": (3, np.uint64),
+    "i64": (4, np.int64),
+    "f64": (5, np.float64),
+}
+REFERENCE_TYPE_NAMES = {"int": "i32", "long": "i64", "float": "f32", "double": "f64"}
+_NP_TO_NAME = {np.dtype(v[1]): k for k, v in DTYPES.items()}
+
+
+class MgsError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"[mgs status {code}] {message}")
+        self.code = code
+
+
+class KernelTime(ctypes.Structure):
+    _fields_ = [("name", ctypes.c_char * 48), ("launches", ctypes.c_uint64), ("total_ms", ctypes.c_double)]
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
+    """Loads libmgs.so (once) and declares the C signatures."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise MgsError(MGS_ERR_INVALID, f"engine library not built: {path} (run __graft_entry__.build())")
+    lib = ctypes.CDLL(path)
+    c_size, c_int, c_void, c_u32 = ctypes.c_size_t, ctypes.c_int, ctypes.c_void_p, ctypes.c_uint32
+    sig = {
+        "mgs_version": ([], c_int),
+        "mgs_last_error_string": ([], ctypes.c_char_p),
+        "mgs_dtype_size": ([c_int], c_size),
+        "mgs_device_count": ([ctypes.POINTER(c_int)], c_int),
+        "mgs_ctx_create": ([c_int, c_size, ctypes.POINTER(c_void)], c_int),
+        "mgs_ctx_destroy": ([c_void], c_int),
+        "mgs_ctx_synchronize": ([c_void], c_int),
+        "mgs_ctx_arena_bytes": ([c_void, ctypes.POINTER(c_size)], c_int),
+        "mgs_ctx_set_profiling": ([c_void, c_int], c_int),
+        "mgs_ctx_kernel_times": ([c_void, ctypes.POINTER(KernelTime), c_int, ctypes.POINTER(c_int)], c_int),
+        "mgs_ctx_launch_count": ([c_void, ctypes.POINTER(ctypes.c_uint64), c_int], c_int),
+        "mgs_host_alloc": ([c_size, ctypes.POINTER(c_void)], c_int),
+        "mgs_host_free": ([c_void], c_int),
+        "mgs_sort_temp_bytes": ([c_int, c_size, ctypes.POINTER(c_size)], c_int),
+        "mgs_sort_device": ([c_void, c_int, c_void, c_size, c_void, c_size, c_void], c_int),
+        "mgs_sort_host": ([c_void, c_int, c_void, c_size], c_int),
+        "mgs_generate": ([c_int, ctypes.c_char_p, c_u32, c_void, c_size], c_int),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = res
+    _lib = lib
+    return lib
+
+
+def _check(rc: int) -> None:
+    if rc != MGS_OK:
+        msg = _lib.mgs_last_error_string()
+        raise MgsError(rc, msg.decode() if msg else "")
+
+
+def dtype_code(dtype) -> int:
+    """Accepts 'u32'..'f64', reference names ('int', 'long', ...) or numpy dtypes."""
+    if isinstance(dtype, str):
+        dtype = REFERENCE_TYPE_NAMES.get(dtype, dtype)
+        return DTYPES[dtype][0]
+    return DTYPES[_NP_TO_NAME[np.dtype(dtype)]][0]
+
+
+def np_dtype(dtype) -> np.dtype:
+    if isinstance(dtype, str):
+        dtype = REFERENCE_TYPE_NAMES.get(dtype, dtype)
+        return np.dtype(DTYPES[dtype][1])
+    return np.dtype(dtype)
+
+
+def device_count() -> int:
+    lib = load_library()
+    c = ctypes.c_int(0)
+    rc = lib.mgs_device_count(ctypes.byref(c))
+    return c.value if rc == MGS_OK else 0
+
+
+def host_empty(n: int, dtype) -> np.ndarray:
+    """A numpy array backed by pinned host memory (HostVector<T>, src/host_vector.cuh:7)."""
+    lib = load_library()
+    dt = np_dtype(dtype)
+    nbytes = max(int(n) * dt.itemsize, 1)
+    p = ctypes.c_void_p()
+    _check(lib.mgs_host_alloc(nbytes, ctypes.byref(p)))
+    buf = (ctypes.c_char * nbytes).from_address(p.value)
+    arr = np.frombuffer(buf, dtype=dt, count=int(n))
+    weakref.finalize(buf, lib.mgs_host_free, ctypes.c_void_p(p.value))
+    return arr
+
+
+def generate(dtype, distribution: str, seed: int, n: int, out: np.ndarray | None = None) -> np.ndarray:
+    """DataGenerator(seed).ComputeDistribution<T>(out, n, distribution) (src/data_generator.cuh:18-36)."""
+    lib = load_library()
+    dt = np_dtype(dtype)
+    if out is None:
+        out = np.zeros(int(n), dtype=dt)
+    assert out.dtype == dt and out.flags.c_contiguous and out.size >= n
+    _check(lib.mgs_generate(dtype_code(dtype), distribution.encode(), int(seed) & 0xFFFFFFFF,
+                            out.ctypes.data_as(ctypes.c_void_p), int(n)))
+    return out
+
+
+class DataGenerator:
+    """Mirror of the reference's DataGenerator (src/data_generator.cuh:12-211)."""
+
+    def __init__(self, distribution_seed: int):
+        self.distribution_seed = int(distribution_seed) & 0xFFFFFFFF
+
+    def compute_distribution(self, begin: np.ndarray, num_elements: int, distribution_type: str) -> None:
+        generate(begin.dtype, distribution_type, self.distribution_seed, num_elements, out=begin)
+
+
+class Context:
+    """One engine context per device (streams, device arena, status word)."""
+
+    def __init__(self, device: int = 0, arena_bytes: int = 0):
+        self._lib = load_library()
+        h = ctypes.c_void_p()
+        _check(self._lib.mgs_ctx_create(int(device), int(arena_bytes), ctypes.byref(h)))
+        self.handle = h
+        self.device = device
+        self._fin = weakref.finalize(self, self._lib.mgs_ctx_destroy, h)
+
+    def close(self) -> None:
+        if self._fin.alive:
+            self._fin()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # --- device-resident sort (thrust::sort on one GPU) ---
+    @staticmethod
+    def sort_temp_bytes(dtype, n: int) -> int:
+        lib = load_library()
+        b = ctypes.c_size_t()
+        _check(lib.mgs_sort_temp_bytes(dtype_code(dtype), int(n), ctypes.byref(b)))
+        return b.value
+
+    def sort_device(self, d_keys: int, n: int, dtype, d_temp: int = 0, temp_bytes: int = 0,
+                    stream: int = 0) -> None:
+        _check(self._lib.mgs_sort_device(self.handle, dtype_code(dtype), ctypes.c_void_p(d_keys), int(n),
+                                         ctypes.c_void_p(d_temp or None), int(temp_bytes),
+                                         ctypes.c_void_p(stream or None)))
+
+    # --- TanasicSort with one GPU: host buffer in, sorted in place ---
+    def sort_host(self, keys: np.ndarray) -> None:
+        assert keys.flags.c_contiguous
+        _check(self._lib.mgs_sort_host(self.handle, dtype_code(keys.dtype), keys.ctypes.data_as(ctypes.c_void_p),
+                                       keys.size))
+
+    def synchronize(self) -> None:
+        _check(self._lib.mgs_ctx_synchronize(self.handle))
+
+    def arena_bytes(self) -> int:
+        b = ctypes.c_size_t()
+        _check(self._lib.mgs_ctx_arena_bytes(self.handle, ctypes.byref(b)))
+        return b.value
+
+    def set_profiling(self, enabled: bool) -> None:
+        _check(self._lib.mgs_ctx_set_profiling(self.handle, 1 if enabled else 0))
+
+    def kernel_times(self) -> dict:
+        cap = 64
+        arr = (KernelTime * cap)()
+        cnt = ctypes.c_int()
+        _check(self._lib.mgs_ctx_kernel_times(self.handle, arr, cap, ctypes.byref(cnt)))
+        return {arr[i].name.decode(): (int(arr[i].launches), float(arr[i].total_ms)) for i in range(min(cnt.value, cap))}
+
+    def launch_count(self, reset: bool = False) -> int:
+        v = ctypes.c_uint64()
+        _check(self._lib.mgs_ctx_launch_count(self.handle, ctypes.byref(v), 1 if reset else 0))
+        return int(v.value)

@@ -1,0 +1,115 @@
+// ORACLE — test infrastructure only. Not part of the product.
+//
+// C entry points around the reference's own code (hpides/multi-gpu-sorting),
+// compiled from the reference's headers where they lie (see oracle/Makefile)
+// into oracle/_ref/libref.so. Each function calls the reference's code path
+// unchanged:
+//   ref_generate          DataGenerator::ComputeDistribution<T>   src/data_generator.cuh:18-36
+//   ref_tanasic_sort      SetupTanasicSort + TanasicSort<T>        src/tanasic_sort.cuh:206-299
+//   ref_gowanlock_sort    SetupGowanlockSort + GowanlockSort<T>    src/gowanlock_sort.cuh:117-125,395-483
+//   ref_gnu_parallel_sort the "gnu_parallel" algorithm branch      src/sort_benchmark.cu:314-319
+//   ref_multiway_merge    __gnu_parallel::multiway_merge call      src/local_cpu_multiway_merge_benchmark.cu:255-256
+//   ref_sort_phase_seconds TimeDurations "sort_phase"              src/time_durations.cuh
+#include <omp.h>
+
+#include <cstdint>
+#include <cstring>
+#include <parallel/algorithm>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "data_generator.cuh"
+#include "gowanlock_sort.cuh"
+#include "host_vector.cuh"
+#include "tanasic_sort.cuh"
+#include "time_durations.cuh"
+
+namespace {
+
+template <typename Fn>
+int dispatch(int dtype, Fn&& fn) {
+  switch (dtype) {
+    case 0: fn(uint32_t{}); return 0;
+    case 1: fn(int{}); return 0;
+    case 2: fn(float{}); return 0;
+    case 3: fn(uint64_t{}); return 0;
+    case 4: fn(long{}); return 0;
+    case 5: fn(double{}); return 0;
+    default: return 1;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int ref_generate(int dtype, const char* distribution, uint32_t seed, void* out, size_t n) {
+  return dispatch(dtype, [&](auto tag) {
+    using T = decltype(tag);
+    DataGenerator generator(seed);
+    // Value-initialised like the benchmark's HostVector input (src/sort_benchmark.cu:280); a plain
+    // vector so that generation needs no CUDA driver.
+    std::vector<T> elements(n);
+    if (n > 0) generator.ComputeDistribution<T>(elements.data(), elements.size(), distribution);
+    if (n > 0) std::memcpy(out, elements.data(), n * sizeof(T));
+  });
+}
+
+int ref_tanasic_sort(int dtype, void* keys, size_t n, int device) {
+  return dispatch(dtype, [&](auto tag) {
+    using T = decltype(tag);
+    std::vector<int> gpus{device};
+    HostVector<T> elements(static_cast<T*>(keys), static_cast<T*>(keys) + n);
+    SetupTanasicSort(gpus);
+    TanasicSort<T>(&elements, gpus);
+    if (n > 0) std::memcpy(keys, thrust::raw_pointer_cast(elements.data()), n * sizeof(T));
+  });
+}
+
+int ref_gowanlock_sort(int dtype, void* keys, size_t n, size_t chunk_size, size_t merge_group_size,
+                       size_t num_buffers, int device, int num_threads) {
+  return dispatch(dtype, [&](auto tag) {
+    using T = decltype(tag);
+    std::vector<int> gpus{device};
+    HostVector<T> elements(static_cast<T*>(keys), static_cast<T*>(keys) + n);
+    SetupGowanlockSort(gpus, num_threads);
+    GowanlockSort<T>(&elements, chunk_size, merge_group_size, num_buffers, gpus);
+    if (n > 0) std::memcpy(keys, thrust::raw_pointer_cast(elements.data()), n * sizeof(T));
+  });
+}
+
+int ref_gnu_parallel_sort(int dtype, void* keys, size_t n, int num_threads) {
+  return dispatch(dtype, [&](auto tag) {
+    using T = decltype(tag);
+    T* p = static_cast<T*>(keys);
+    omp_set_num_threads(num_threads);
+    TimeDurations::Get()->Tic("sort_phase");
+    __gnu_parallel::sort(p, p + n);
+    TimeDurations::Get()->Toc("sort_phase");
+  });
+}
+
+int ref_multiway_merge(int dtype, const void* const* runs, const size_t* lens, int k, void* out, int num_threads) {
+  return dispatch(dtype, [&](auto tag) {
+    using T = decltype(tag);
+    omp_set_num_threads(num_threads);
+    std::vector<std::pair<T*, T*>> iterator_pairs;
+    size_t total = 0;
+    for (int i = 0; i < k; ++i) {
+      T* b = const_cast<T*>(static_cast<const T*>(runs[i]));
+      iterator_pairs.emplace_back(b, b + lens[i]);
+      total += lens[i];
+    }
+    TimeDurations::Get()->Tic("merge_phase");
+    __gnu_parallel::multiway_merge(iterator_pairs.begin(), iterator_pairs.end(), static_cast<T*>(out), total,
+                                   std::less<T>());
+    TimeDurations::Get()->Toc("merge_phase");
+  });
+}
+
+double ref_phase_seconds(const char* phase) { return TimeDurations::Get()->durations[phase].count(); }
+
+int ref_num_procs(void) { return omp_get_num_procs(); }
+
+}  // extern "C"
