@@ -273,7 +273,7 @@ def main():
         t = torch.tensor([e2e_s], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
-    e2e_value = world * n * len(e2e_times) / e2e_s
+    e2e_value = world * n * len(e2e_times) / e2e_s if e2e_times else None
 
     peak, peak_kind = measured_hbm_peak()
     one = ktimes.get("radix_onesweep", (0, 0.0))

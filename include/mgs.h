@@ -111,6 +111,39 @@ int mgs_sort_device(mgs_ctx* ctx, int dtype, void* d_keys, size_t n, void* d_tem
  * reference (src/tanasic_sort.cuh:225-227). */
 int mgs_sort_host(mgs_ctx* ctx, int dtype, void* h_keys, size_t n);
 
+/* ---- TanasicSort with g partitions as chunks of one GPU --------------------
+ * (src/tanasic_sort.cuh:223-299 with MergePartitions :176-204). The reference's
+ * per-GPU partitions become num_chunks (a power of two, <= 128) chunks of this
+ * GPU's HBM; the pivot search (FindPivot :45-87), the exchange of the pivot
+ * ranges (SwapPartitions :89-146) and the boundary merges
+ * (MergeLocalPartitions :148-174) run between those chunks. n is padded to a
+ * multiple of num_chunks with the type's maximum like the reference
+ * (:231-238,255-259), including its effect on +inf / NaN keys (the padding
+ * sorts before them and the copy-back keeps the padding). num_chunks == 1 is
+ * mgs_sort_host. Synchronous. */
+int mgs_tanasic_sort(mgs_ctx* ctx, int dtype, void* h_keys, size_t n, int num_chunks);
+/* Same on a device buffer (in/out), using the context arena. Synchronous. */
+int mgs_tanasic_sort_device(mgs_ctx* ctx, int dtype, void* d_keys, size_t n, int num_chunks);
+
+/* ---- merge-path pivot (SelectPivot/FindPivot, src/tanasic_sort.cuh:15-87) ----
+ * d_left/d_right: host arrays of `half` device pointers to sorted chunks of
+ * chunk_size keys. Returns the largest p with left[N-p] > right[p-1] over the
+ * virtual concatenations (N = half * chunk_size). Synchronous. */
+int mgs_find_pivot_device(mgs_ctx* ctx, int dtype, const void* const* d_left, const void* const* d_right, int half,
+                          size_t chunk_size, size_t* pivot);
+
+/* ---- merges ---------------------------------------------------------------
+ * thrust::merge of two sorted device ranges (src/tanasic_sort.cuh:163-167):
+ * stable, on equal keys the first range first. k-way merge of k sorted device
+ * runs (HET sort's __gnu_parallel::multiway_merge, src/gowanlock_sort.cuh:73-74,
+ * 91-92): stable by run index, k <= 1024. d_runs and lens are host arrays.
+ * d_temp may be NULL (context arena). Asynchronous on `stream`. */
+int mgs_merge_temp_bytes(int dtype, int k, size_t total, size_t* bytes);
+int mgs_merge_device(mgs_ctx* ctx, int dtype, const void* d_a, size_t na, const void* d_b, size_t nb, void* d_out,
+                     void* d_temp, size_t temp_bytes, void* stream);
+int mgs_kway_merge_device(mgs_ctx* ctx, int dtype, const void* const* d_runs, const size_t* lens, int k, void* d_out,
+                          void* d_temp, size_t temp_bytes, void* stream);
+
 /* ---- DataGenerator::ComputeDistribution<T> (src/data_generator.cuh:18-36) ----
  * Fills the host buffer out[0..n) exactly as the reference generator does for
  * the reference's distributions: "uniform", "normal", "zero", "staggered",

@@ -10,7 +10,9 @@
 #include <string>
 
 #include "../kernels/engine_types.h"
+#include "../kernels/merge.cuh"
 #include "../kernels/radix_sort.cuh"
+#include "chunk_sort.h"
 #include "context.h"
 
 namespace mgs {
@@ -107,6 +109,7 @@ int mgs_ctx_create(int device, size_t arena_bytes, mgs_ctx** out) {
   if (e == cudaSuccess) e = cudaMalloc(&c.d_status, 256);
   if (e == cudaSuccess) e = cudaMemset(c.d_status, 0, 256);
   if (e == cudaSuccess) e = cudaMallocHost(&c.h_status, 256);
+  if (e == cudaSuccess) c.h_status64 = reinterpret_cast<uint64_t*>(reinterpret_cast<char*>(c.h_status) + 64);
   if (e == cudaSuccess && arena_bytes > 0) e = c.reserve(arena_bytes);
   if (e != cudaSuccess) {
     int rc = cuda_fail(e, "mgs_ctx_create");
@@ -273,6 +276,126 @@ int mgs_sort_host(mgs_ctx* ctx, int dtype, void* h_keys, size_t n) {
   int rc = status_to_code(status);
   if (rc == MGS_OK) mgs::clear_last_error();
   return rc;
+}
+
+static int finish_sync(Context& c, const char* what) {
+  uint32_t status = 0;
+  cudaError_t e = c.take_status(c.compute, &status);
+  if (e != cudaSuccess) return cuda_fail(e, what);
+  int rc = status_to_code(status);
+  if (rc == MGS_OK) mgs::clear_last_error();
+  return rc;
+}
+
+static int check_chunks(int num_chunks) {
+  if (num_chunks < 1 || (num_chunks & (num_chunks - 1)) != 0 || num_chunks > 2 * mgs::kMaxPivotHalf) return 0;
+  return 1;
+}
+
+int mgs_tanasic_sort(mgs_ctx* ctx, int dtype, void* h_keys, size_t n, int num_chunks) {
+  if (!ctx) return invalid("mgs_tanasic_sort: ctx is null");
+  if (mgs::dtype_bytes(dtype) == 0) return invalid("mgs_tanasic_sort: unknown dtype");
+  if (!check_chunks(num_chunks)) return invalid("mgs_tanasic_sort: num_chunks must be a power of two in [1, 128]");
+  if (n == 0) return MGS_OK;  // src/tanasic_sort.cuh:225-227
+  if (!h_keys) return invalid("mgs_tanasic_sort: h_keys is null");
+  if (num_chunks == 1) return mgs_sort_host(ctx, dtype, h_keys, n);
+  Context& c = ctx->impl;
+  DeviceGuard g(c.device);
+  const mgs::ChunkPlan plan = mgs::plan_chunks(n, num_chunks);
+  if (plan.chunk > kMaxDeviceSortKeys) return invalid("mgs_tanasic_sort: chunks must hold fewer than 2^32 keys");
+  const size_t temp = mgs::chunk_sort_temp_bytes(dtype, n, num_chunks);
+  cudaError_t e = c.reserve(temp);
+  if (e != cudaSuccess) return cuda_fail(e, "mgs_tanasic_sort: arena");
+  e = mgs::chunk_sort(c, dtype, h_keys, h_keys, nullptr, n, num_chunks, c.arena, c.arena_bytes, c.compute);
+  if (e != cudaSuccess) return cuda_fail(e, "mgs_tanasic_sort");
+  return finish_sync(c, "mgs_tanasic_sort: synchronize");
+}
+
+int mgs_tanasic_sort_device(mgs_ctx* ctx, int dtype, void* d_keys, size_t n, int num_chunks) {
+  if (!ctx) return invalid("mgs_tanasic_sort_device: ctx is null");
+  const size_t w = mgs::dtype_bytes(dtype);
+  if (w == 0) return invalid("mgs_tanasic_sort_device: unknown dtype");
+  if (!check_chunks(num_chunks)) return invalid("mgs_tanasic_sort_device: num_chunks must be a power of two in [1, 128]");
+  if (n == 0) return MGS_OK;
+  if (!d_keys) return invalid("mgs_tanasic_sort_device: d_keys is null");
+  Context& c = ctx->impl;
+  DeviceGuard g(c.device);
+  const mgs::ChunkPlan plan = mgs::plan_chunks(n, num_chunks);
+  if (plan.chunk > kMaxDeviceSortKeys) return invalid("mgs_tanasic_sort_device: chunks must hold fewer than 2^32 keys");
+  const size_t temp = mgs::chunk_sort_temp_bytes(dtype, n, num_chunks);
+  cudaError_t e = c.reserve(temp);
+  if (e != cudaSuccess) return cuda_fail(e, "mgs_tanasic_sort_device: arena");
+  e = mgs::chunk_sort(c, dtype, nullptr, nullptr, d_keys, n, num_chunks, c.arena, c.arena_bytes, c.compute);
+  if (e != cudaSuccess) return cuda_fail(e, "mgs_tanasic_sort_device");
+  return finish_sync(c, "mgs_tanasic_sort_device: synchronize");
+}
+
+int mgs_find_pivot_device(mgs_ctx* ctx, int dtype, const void* const* d_left, const void* const* d_right, int half,
+                          size_t chunk_size, size_t* pivot) {
+  if (!ctx || !d_left || !d_right || !pivot) return invalid("mgs_find_pivot_device: null argument");
+  if (mgs::dtype_bytes(dtype) == 0) return invalid("mgs_find_pivot_device: unknown dtype");
+  if (half < 1 || half > mgs::kMaxPivotHalf || chunk_size == 0)
+    return invalid("mgs_find_pivot_device: half must be in [1, 64] and chunk_size > 0");
+  Context& c = ctx->impl;
+  DeviceGuard g(c.device);
+  cudaError_t e = c.reserve(256);
+  if (e != cudaSuccess) return cuda_fail(e, "mgs_find_pivot_device: arena");
+  uint64_t* d_pivot = static_cast<uint64_t*>(c.arena);
+  e = mgs::pivot_search(dtype, d_left, d_right, half, chunk_size, d_pivot, c.compute, &c.recorder);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(c.h_status64, d_pivot, 8, cudaMemcpyDeviceToHost, c.compute);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c.compute);
+  if (e != cudaSuccess) return cuda_fail(e, "mgs_find_pivot_device");
+  *pivot = size_t(*c.h_status64);
+  mgs::clear_last_error();
+  return MGS_OK;
+}
+
+int mgs_merge_temp_bytes(int dtype, int k, size_t total, size_t* bytes) {
+  if (!bytes) return invalid("mgs_merge_temp_bytes: bytes is null");
+  if (mgs::dtype_bytes(dtype) == 0) return invalid("mgs_merge_temp_bytes: unknown dtype");
+  if (k < 1 || k > mgs::kMaxKwayRuns) return invalid("mgs_merge_temp_bytes: k must be in [1, 1024]");
+  *bytes = mgs::kway_merge_temp_bytes(dtype, k, total);
+  return MGS_OK;
+}
+
+int mgs_kway_merge_device(mgs_ctx* ctx, int dtype, const void* const* d_runs, const size_t* lens, int k, void* d_out,
+                          void* d_temp, size_t temp_bytes, void* stream) {
+  if (!ctx) return invalid("mgs_kway_merge_device: ctx is null");
+  const size_t w = mgs::dtype_bytes(dtype);
+  if (w == 0) return invalid("mgs_kway_merge_device: unknown dtype");
+  if (k < 1 || k > mgs::kMaxKwayRuns) return invalid("mgs_kway_merge_device: k must be in [1, 1024]");
+  if (!d_runs || !lens) return invalid("mgs_kway_merge_device: null run table");
+  size_t total = 0;
+  for (int r = 0; r < k; ++r) {
+    if (lens[r] > 0 && !d_runs[r]) return invalid("mgs_kway_merge_device: null run pointer");
+    total += lens[r];
+  }
+  if (total == 0) return MGS_OK;
+  if (!d_out) return invalid("mgs_kway_merge_device: d_out is null");
+  Context& c = ctx->impl;
+  DeviceGuard g(c.device);
+  const size_t need = mgs::kway_merge_temp_bytes(dtype, k, total);
+  if (d_temp == nullptr) {
+    cudaError_t e = c.reserve(need);
+    if (e != cudaSuccess) return cuda_fail(e, "mgs_kway_merge_device: arena");
+    d_temp = c.arena;
+    temp_bytes = c.arena_bytes;
+  } else if (temp_bytes < need) {
+    set_last_error("mgs_kway_merge_device: d_temp holds %zu bytes, %zu needed", temp_bytes, need);
+    return MGS_ERR_INVALID;
+  }
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c.compute;
+  cudaError_t e = mgs::kway_merge(dtype, d_runs, lens, k, d_out, d_temp, temp_bytes, s, &c.recorder);
+  if (e != cudaSuccess) return cuda_fail(e, "mgs_kway_merge_device");
+  mgs::clear_last_error();
+  return MGS_OK;
+}
+
+int mgs_merge_device(mgs_ctx* ctx, int dtype, const void* d_a, size_t na, const void* d_b, size_t nb, void* d_out,
+                     void* d_temp, size_t temp_bytes, void* stream) {
+  const void* runs[2] = {d_a, d_b};
+  const size_t lens[2] = {na, nb};
+  return mgs_kway_merge_device(ctx, dtype, runs, lens, 2, d_out, d_temp, temp_bytes, stream);
 }
 
 int mgs_generate(int dtype, const char* distribution, uint32_t seed, void* out, size_t n) {

@@ -55,6 +55,7 @@ struct Context {
   size_t arena_bytes = 0;
   uint32_t* d_status = nullptr;  // device status word (DeviceStatus bits)
   uint32_t* h_status = nullptr;  // pinned mirror used by status reads
+  uint64_t* h_status64 = nullptr;  // pinned 8-byte word (pivot readback), inside the h_status block
   EventRecorder recorder;
 
   // Ensures the arena holds at least `bytes` (synchronizes before growing).

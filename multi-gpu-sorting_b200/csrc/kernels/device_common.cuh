@@ -50,6 +50,12 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
   return m;
 }
 
+__device__ __forceinline__ uint32_t lanemask_gt() {
+  uint32_t m;
+  asm volatile("mov.u32 %0, %%lanemask_gt;" : "=r"(m));
+  return m;
+}
+
 __device__ __forceinline__ uint32_t ld_volatile_u32(const uint32_t* p) {
   uint32_t v;
   asm volatile("ld.volatile.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");

@@ -1,0 +1,517 @@
+// Merge kernels for one B200 (sm_100a).
+//
+//   K3 pivot_search    : SelectPivot/FindPivot of P2P sort (src/tanasic_sort.cuh:
+//                        15-87) as one warp doing a 32-ary search over the
+//                        virtual concatenations of the left and right chunks
+//                        (about log32(N) dependent rounds instead of log2(N)).
+//   K4 merge_partition : merge-path diagonal search for a two-way merge, one
+//                        thread per output tile boundary.
+//   K7a kway_partition : exact multi-sequence selection for a k-way merge, one
+//                        warp per output tile boundary: bisection over the radix
+//                        order key space, every lane narrowing the index window of
+//                        its runs, then ties split by run index (stable).
+//                        Hierarchical: a coarse level bounds the fine searches.
+//   K5/K7b tile_merge  : per output tile, the k input ranges are staged in shared
+//                        memory in run order and merged by ceil(log2 k) rounds of
+//                        pairwise merge-path merges in shared memory, then stored
+//                        coalesced. k = 2 is thrust::merge (src/tanasic_sort.cuh:
+//                        163-167); k > 2 replaces __gnu_parallel::multiway_merge
+//                        (src/gowanlock_sort.cuh:73-74,91-92).
+// Order: radix order of the keys (KeyTraits::Ordered); on ties the lower run
+// (the first range) comes first.
+#include <algorithm>
+#include <mutex>
+#include <vector>
+
+#include "device_common.cuh"
+#include "dispatch.cuh"
+#include "merge.cuh"
+
+namespace mgs {
+namespace {
+
+using u64 = unsigned long long;
+
+template <typename Bits>
+struct ChunkTable {
+  const Bits* left[kMaxPivotHalf];
+  const Bits* right[kMaxPivotHalf];
+};
+
+// ---------------------------------------------------------------- K3 --------
+template <class Tr>
+__global__ __launch_bounds__(32) void pivot_search_kernel(ChunkTable<typename Tr::Bits> tab, int half, u64 psize,
+                                                          u64* __restrict__ out) {
+  const int lane = threadIdx.x;
+  const u64 N = psize * u64(half);
+  auto L = [&](u64 i) { return tab.left[i / psize][i % psize]; };
+  auto R = [&](u64 i) { return tab.right[i / psize][i % psize]; };
+  // f(p) = left[N - p] > right[p - 1] is true exactly for p <= pivot.
+  u64 lo = 0, hi = N;
+  while (lo < hi) {
+    const u64 step = (hi - lo + 31) / 32;
+    const u64 p = min(lo + u64(lane + 1) * step, hi);
+    const bool t = Tr::Less(R(p - 1), L(N - p));
+    const uint32_t bal = __ballot_sync(0xffffffffu, t);
+    const int c = __popc(bal);
+    if (c == 0) {
+      hi = lo + step - 1;
+    } else {
+      const u64 nlo = min(lo + u64(c) * step, hi);
+      const u64 nhi = (c < 32) ? min(lo + u64(c + 1) * step, hi) - 1 : hi;
+      lo = nlo;
+      hi = nhi;
+    }
+  }
+  if (lane == 0) *out = lo;
+}
+
+// ---------------------------------------------------------------- K4 --------
+template <class Tr>
+__global__ __launch_bounds__(256) void merge_partition_kernel(const typename Tr::Bits* __restrict__ a, u64 na,
+                                                              const typename Tr::Bits* __restrict__ b, u64 nb,
+                                                              u64 spacing, u64 num_diag, u64* __restrict__ splits) {
+  const u64 j = u64(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (j >= num_diag) return;
+  const u64 d = min(j * spacing, na + nb);
+  u64 lo = d > nb ? d - nb : 0, hi = min(d, na);
+  while (lo < hi) {
+    const u64 mid = (lo + hi) / 2;
+    if (!Tr::Less(b[d - 1 - mid], a[mid])) {
+      lo = mid + 1;
+    } else {
+      hi = mid;
+    }
+  }
+  splits[2 * j] = lo;
+  splits[2 * j + 1] = d - lo;
+}
+
+// ---------------------------------------------------------------- K7a -------
+template <typename Bits>
+__device__ __forceinline__ u64 warp_sum_u64(u64 v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// First index in [lo, hi) whose radix-order key is > v (upper) or >= v (lower).
+template <class Tr, bool UPPER>
+__device__ __forceinline__ u64 bound_search(const typename Tr::Bits* run, u64 lo, u64 hi, typename Tr::Bits v) {
+  while (lo < hi) {
+    const u64 mid = (lo + hi) / 2;
+    const typename Tr::Bits o = Tr::Ordered(run[mid]);
+    if (UPPER ? (o <= v) : (o < v)) {
+      lo = mid + 1;
+    } else {
+      hi = mid;
+    }
+  }
+  return lo;
+}
+
+constexpr int kMaxRunsPerLane = kMaxKwayRuns / 32;
+
+// One warp per diagonal d: splits[r] = number of elements of run r among the
+// first d outputs of the stable k-way merge. Optional coarse level: the
+// splits / ub / lt / v* of the enclosing coarse diagonals bound the search.
+template <class Tr>
+__global__ __launch_bounds__(128) void kway_partition_kernel(
+    const typename Tr::Bits* const* __restrict__ runs, const u64* __restrict__ lens, int k, u64 total, u64 spacing,
+    u64 num_diag, const u64* __restrict__ c_splits, const u64* __restrict__ c_ub, const u64* __restrict__ c_lt,
+    const typename Tr::Bits* __restrict__ c_vstar, u64 c_spacing, u64* __restrict__ splits, u64* __restrict__ ub_out,
+    u64* __restrict__ lt_out, typename Tr::Bits* __restrict__ vstar_out) {
+  using Bits = typename Tr::Bits;
+  const u64 w = (u64(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (w >= num_diag) return;
+  const u64 d = min(w * spacing, total);
+  const int per_lane = (k + 31) / 32;
+  if (d >= total) {
+    for (int i = 0; i < per_lane; ++i) {
+      const int r = lane + 32 * i;
+      if (r < k) {
+        splits[w * k + r] = lens[r];
+        if (ub_out) ub_out[w * k + r] = lens[r];
+        if (lt_out) lt_out[w * k + r] = lens[r];
+      }
+    }
+    if (vstar_out && lane == 0) vstar_out[w] = ~Bits(0);
+    return;
+  }
+  u64 a[kMaxRunsPerLane], b[kMaxRunsPerLane], base[kMaxRunsPerLane];
+  Bits vlo = 0, vhi = ~Bits(0);
+  u64 c0 = 0, c1 = 0;
+  if (c_splits) {
+    c0 = d / c_spacing;
+    c1 = c0 + 1;
+    vlo = c_vstar[c0];
+    vhi = c_vstar[c1];
+  }
+  for (int i = 0; i < per_lane; ++i) {
+    const int r = lane + 32 * i;
+    if (r < k) {
+      a[i] = c_splits ? c_splits[c0 * k + r] : 0;
+      base[i] = c_splits ? c_lt[c0 * k + r] : 0;
+      b[i] = c_splits ? c_ub[c1 * k + r] : lens[r];
+    } else {
+      a[i] = b[i] = base[i] = 0;
+    }
+  }
+  // Bisection for v* = the smallest v with (number of keys <= v) > d.
+  while (vlo < vhi) {
+    u64 width = 0;
+    for (int i = 0; i < per_lane; ++i) width += b[i] - a[i];
+    if (warp_sum_u64<Bits>(width) == 0) break;  // no key strictly inside: v* = vlo
+    const Bits vmid = vlo + (vhi - vlo) / 2;
+    u64 u[kMaxRunsPerLane];
+    u64 cnt = 0;
+    for (int i = 0; i < per_lane; ++i) {
+      const int r = lane + 32 * i;
+      u[i] = (r < k) ? bound_search<Tr, true>(runs[r], a[i], b[i], vmid) : 0;
+      cnt += u[i];
+    }
+    const u64 le = warp_sum_u64<Bits>(cnt);
+    if (le > d) {
+      vhi = vmid;
+      for (int i = 0; i < per_lane; ++i) b[i] = u[i];
+    } else {
+      vlo = vmid + 1;
+      for (int i = 0; i < per_lane; ++i) a[i] = base[i] = u[i];
+    }
+  }
+  const Bits vs = vlo;
+  // Keys equal to v* are split across runs in run order (stability).
+  u64 lt[kMaxRunsPerLane], eq[kMaxRunsPerLane];
+  u64 lt_sum = 0;
+  for (int i = 0; i < per_lane; ++i) {
+    const int r = lane + 32 * i;
+    if (r < k) {
+      lt[i] = bound_search<Tr, false>(runs[r], base[i], b[i], vs);
+      const u64 ubr = bound_search<Tr, true>(runs[r], max(a[i], lt[i]), b[i], vs);
+      eq[i] = ubr - lt[i];
+      if (ub_out) ub_out[w * k + r] = ubr;
+      if (lt_out) lt_out[w * k + r] = lt[i];
+    } else {
+      lt[i] = eq[i] = 0;
+    }
+    lt_sum += lt[i];
+  }
+  const u64 rem = d - warp_sum_u64<Bits>(lt_sum);
+  u64 before = 0;  // equal keys in all runs with a lower index
+  for (int i = 0; i < per_lane; ++i) {
+    u64 incl = eq[i];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const u64 t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    const u64 excl = before + incl - eq[i];
+    const int r = lane + 32 * i;
+    if (r < k) {
+      const u64 take = rem > excl ? min(rem - excl, eq[i]) : 0;
+      splits[w * k + r] = lt[i] + take;
+    }
+    before += __shfl_sync(0xffffffffu, incl, 31);
+  }
+  if (vstar_out && lane == 0) vstar_out[w] = vs;
+}
+
+// ---------------------------------------------------------------- K5/K7b ----
+template <class Tr, int BLOCK, int ITEMS>
+__global__ __launch_bounds__(BLOCK) void tile_merge_kernel(const typename Tr::Bits* const* __restrict__ runs, int k,
+                                                           const u64* __restrict__ splits,
+                                                           typename Tr::Bits* __restrict__ out, u64 total) {
+  using Bits = typename Tr::Bits;
+  constexpr int kTile = BLOCK * ITEMS;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Bits* buf0 = reinterpret_cast<Bits*>(smem_raw);
+  Bits* buf1 = buf0 + kTile;
+  u64* sstart = reinterpret_cast<u64*>(buf1 + kTile);
+  uint32_t* seg0 = reinterpret_cast<uint32_t*>(sstart + k);
+  uint32_t* seg1 = seg0 + (k + 1);
+  __shared__ uint32_t scan_tmp[BLOCK / 32 + 1];
+
+  const int tid = threadIdx.x;
+  const u64 j = blockIdx.x;
+  const u64 d0 = j * u64(kTile);
+  const uint32_t cnt = uint32_t(min(u64(kTile), total - d0));
+
+  // Segment offsets of the k input ranges (exclusive scan of their lengths).
+  const int per_thread = (k + BLOCK - 1) / BLOCK;
+  uint32_t local = 0;
+  for (int i = 0; i < per_thread; ++i) {
+    const int r = tid * per_thread + i;
+    if (r < k) {
+      const u64 s = splits[j * k + r];
+      sstart[r] = s;
+      local += uint32_t(splits[(j + 1) * k + r] - s);
+    }
+  }
+  uint32_t tot;
+  uint32_t run_off = block_exclusive_scan<BLOCK>(local, scan_tmp, &tot);
+  for (int i = 0; i < per_thread; ++i) {
+    const int r = tid * per_thread + i;
+    if (r < k) {
+      seg0[r] = run_off;
+      run_off += uint32_t(splits[(j + 1) * k + r] - sstart[r]);
+    }
+  }
+  if (tid == 0) seg0[k] = cnt;
+  __syncthreads();
+
+  // Stage the k ranges back to back in run order.
+  for (uint32_t i = tid; i < cnt; i += BLOCK) {
+    int lo = 0, hi = k;  // largest r with seg0[r] <= i
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (seg0[mid] <= i) {
+        lo = mid;
+      } else {
+        hi = mid;
+      }
+    }
+    buf0[i] = runs[lo][sstart[lo] + (i - seg0[lo])];
+  }
+  __syncthreads();
+
+  // Pairwise merge rounds in shared memory.
+  Bits* src = buf0;
+  Bits* dst = buf1;
+  uint32_t* so = seg0;
+  uint32_t* no = seg1;
+  int m = k;
+  while (m > 1) {
+    const int m2 = (m + 1) / 2;
+    for (int i = tid; i <= m2; i += BLOCK) no[i] = (i < m2) ? so[2 * i] : cnt;
+    __syncthreads();
+    uint32_t p = uint32_t(tid) * ITEMS;
+    const uint32_t p1 = min(p + ITEMS, cnt);
+    if (p < p1) {
+      int lo = 0, hi = m2;  // pair containing p: largest q with no[q] <= p
+      while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (no[mid] <= p) {
+          lo = mid;
+        } else {
+          hi = mid;
+        }
+      }
+      int q = lo;
+      while (p < p1) {
+        const uint32_t a0 = so[2 * q];
+        const uint32_t a1 = so[min(2 * q + 1, m)];
+        const uint32_t b1 = so[min(2 * q + 2, m)];
+        const Bits* A = src + a0;
+        const Bits* B = src + a1;
+        const uint32_t la = a1 - a0, lb = b1 - a1;
+        const uint32_t diag = p - a0;
+        uint32_t s_lo = diag > lb ? diag - lb : 0, s_hi = min(diag, la);
+        while (s_lo < s_hi) {
+          const uint32_t mid = (s_lo + s_hi) >> 1;
+          if (!Tr::Less(B[diag - 1 - mid], A[mid])) {
+            s_lo = mid + 1;
+          } else {
+            s_hi = mid;
+          }
+        }
+        uint32_t ia = s_lo, ib = diag - s_lo;
+        Bits va = ia < la ? A[ia] : Bits(0);
+        Bits vb = ib < lb ? B[ib] : Bits(0);
+        const uint32_t pend = min(p1, b1);
+        while (p < pend) {
+          const bool take_b = ib < lb && (ia >= la || Tr::Less(vb, va));
+          if (take_b) {
+            dst[p++] = vb;
+            ++ib;
+            if (ib < lb) vb = B[ib];
+          } else {
+            dst[p++] = va;
+            ++ia;
+            if (ia < la) va = A[ia];
+          }
+        }
+        ++q;
+      }
+    }
+    __syncthreads();
+    Bits* t = src;
+    src = dst;
+    dst = t;
+    uint32_t* ts = so;
+    so = no;
+    no = ts;
+    m = m2;
+  }
+
+  for (uint32_t i = tid; i < cnt; i += BLOCK) out[d0 + i] = src[i];
+}
+
+// ---------------------------------------------------------------- host ------
+size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+template <int KEY_BYTES>
+struct MergeShape;
+template <>
+struct MergeShape<4> {
+  static constexpr int kBlock = 256;
+  static constexpr int kItems = 16;
+};
+template <>
+struct MergeShape<8> {
+  static constexpr int kBlock = 256;
+  static constexpr int kItems = 8;
+};
+
+constexpr u64 kCoarseTiles = 256;  // fine tiles per coarse diagonal
+
+struct KwayLayout {
+  size_t ptrs_off, lens_off, splits_off, c_splits_off, c_ub_off, c_lt_off, c_vstar_off, total;
+  u64 num_tiles, num_coarse;
+  bool coarse;
+};
+
+template <class Tr>
+KwayLayout kway_layout(int k, size_t total) {
+  using Shape = MergeShape<sizeof(typename Tr::Bits)>;
+  constexpr u64 kTile = u64(Shape::kBlock) * Shape::kItems;
+  KwayLayout L;
+  L.num_tiles = (total + kTile - 1) / kTile;
+  L.coarse = (k > 2) && (L.num_tiles > 2 * kCoarseTiles);
+  L.num_coarse = L.coarse ? (total + kTile * kCoarseTiles - 1) / (kTile * kCoarseTiles) : 0;
+  size_t off = 0;
+  L.ptrs_off = off;
+  off += align_up(size_t(k) * 8, 256);
+  L.lens_off = off;
+  off += align_up(size_t(k) * 8, 256);
+  L.splits_off = off;
+  off += align_up(size_t(L.num_tiles + 1) * k * 8, 256);
+  const size_t cn = size_t(L.num_coarse + 1);
+  L.c_splits_off = off;
+  off += L.coarse ? align_up(cn * k * 8, 256) : 0;
+  L.c_ub_off = off;
+  off += L.coarse ? align_up(cn * k * 8, 256) : 0;
+  L.c_lt_off = off;
+  off += L.coarse ? align_up(cn * k * 8, 256) : 0;
+  L.c_vstar_off = off;
+  off += L.coarse ? align_up(cn * sizeof(typename Tr::Bits), 256) : 0;
+  L.total = off;
+  return L;
+}
+
+template <class Tr>
+cudaError_t kway_merge_typed(const void* const* runs_v, const size_t* lens, int k, void* out_v, void* temp,
+                             size_t temp_bytes, cudaStream_t stream, LaunchRecorder* rec) {
+  using Bits = typename Tr::Bits;
+  using Shape = MergeShape<sizeof(Bits)>;
+  constexpr u64 kTile = u64(Shape::kBlock) * Shape::kItems;
+  if (k <= 0 || k > kMaxKwayRuns) return cudaErrorInvalidValue;
+  size_t total = 0;
+  for (int r = 0; r < k; ++r) total += lens[r];
+  if (total == 0) return cudaSuccess;
+  Bits* out = static_cast<Bits*>(out_v);
+  if (k == 1) return cudaMemcpyAsync(out, runs_v[0], lens[0] * sizeof(Bits), cudaMemcpyDeviceToDevice, stream);
+  const KwayLayout L = kway_layout<Tr>(k, total);
+  if (temp == nullptr || temp_bytes < L.total) return cudaErrorInvalidValue;
+  char* tb = static_cast<char*>(temp);
+  const Bits** d_runs = reinterpret_cast<const Bits**>(tb + L.ptrs_off);
+  u64* d_lens = reinterpret_cast<u64*>(tb + L.lens_off);
+  u64* d_splits = reinterpret_cast<u64*>(tb + L.splits_off);
+  {
+    // Pageable-source copies are staged by the runtime before the call returns.
+    std::vector<u64> hp(k), hl(k);
+    for (int r = 0; r < k; ++r) {
+      hp[r] = reinterpret_cast<u64>(runs_v[r]);
+      hl[r] = lens[r];
+    }
+    cudaError_t e = cudaMemcpyAsync(d_runs, hp.data(), size_t(k) * 8, cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_lens, hl.data(), size_t(k) * 8, cudaMemcpyHostToDevice, stream);
+    if (e != cudaSuccess) return e;
+  }
+  const u64 num_diag = L.num_tiles + 1;
+  cudaError_t e;
+  if (k == 2) {
+    e = launch_kernel(rec, "merge_partition", merge_partition_kernel<Tr>, dim3(unsigned((num_diag + 255) / 256)),
+                      dim3(256), 0, stream, static_cast<const Bits*>(runs_v[0]), u64(lens[0]),
+                      static_cast<const Bits*>(runs_v[1]), u64(lens[1]), kTile, num_diag, d_splits);
+  } else {
+    const u64* c_splits = nullptr;
+    const u64* c_ub = nullptr;
+    const u64* c_lt = nullptr;
+    const Bits* c_vstar = nullptr;
+    const u64 c_spacing = kTile * kCoarseTiles;
+    if (L.coarse) {
+      u64* cs = reinterpret_cast<u64*>(tb + L.c_splits_off);
+      u64* cu = reinterpret_cast<u64*>(tb + L.c_ub_off);
+      u64* cl = reinterpret_cast<u64*>(tb + L.c_lt_off);
+      Bits* cv = reinterpret_cast<Bits*>(tb + L.c_vstar_off);
+      const u64 cdiag = L.num_coarse + 1;
+      e = launch_kernel(rec, "kway_partition", kway_partition_kernel<Tr>, dim3(unsigned((cdiag * 32 + 127) / 128)),
+                        dim3(128), 0, stream, d_runs, d_lens, k, u64(total), c_spacing, cdiag,
+                        static_cast<const u64*>(nullptr), static_cast<const u64*>(nullptr),
+                        static_cast<const u64*>(nullptr), static_cast<const Bits*>(nullptr), u64(1), cs, cu, cl, cv);
+      if (e != cudaSuccess) return e;
+      c_splits = cs;
+      c_ub = cu;
+      c_lt = cl;
+      c_vstar = cv;
+    }
+    e = launch_kernel(rec, "kway_partition", kway_partition_kernel<Tr>, dim3(unsigned((num_diag * 32 + 127) / 128)),
+                      dim3(128), 0, stream, d_runs, d_lens, k, u64(total), kTile, num_diag, c_splits, c_ub, c_lt,
+                      c_vstar, c_spacing, d_splits, static_cast<u64*>(nullptr), static_cast<u64*>(nullptr),
+                      static_cast<Bits*>(nullptr));
+  }
+  if (e != cudaSuccess) return e;
+  auto kernel = tile_merge_kernel<Tr, Shape::kBlock, Shape::kItems>;
+  const size_t smem = 2 * kTile * sizeof(Bits) + size_t(k) * 8 + size_t(2 * (k + 1)) * 4;
+  static std::once_flag once;
+  std::call_once(once, [&] {
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         int(2 * kTile * sizeof(Bits) + size_t(kMaxKwayRuns) * 8 + size_t(2 * (kMaxKwayRuns + 1)) * 4));
+  });
+  return launch_kernel(rec, k == 2 ? "merge_tiles" : "kway_merge_tiles", kernel, dim3(unsigned(L.num_tiles)),
+                       dim3(Shape::kBlock), smem, stream, d_runs, k, static_cast<const u64*>(d_splits), out, u64(total));
+}
+
+template <class Tr>
+cudaError_t pivot_search_typed(const void* const* left, const void* const* right, int half, size_t psize,
+                               uint64_t* d_pivot, cudaStream_t stream, LaunchRecorder* rec) {
+  using Bits = typename Tr::Bits;
+  if (half <= 0 || half > kMaxPivotHalf || psize == 0) return cudaErrorInvalidValue;
+  ChunkTable<Bits> tab{};
+  for (int i = 0; i < half; ++i) {
+    tab.left[i] = static_cast<const Bits*>(left[i]);
+    tab.right[i] = static_cast<const Bits*>(right[i]);
+  }
+  return launch_kernel(rec, "pivot_search", pivot_search_kernel<Tr>, dim3(1), dim3(32), 0, stream, tab, half,
+                       u64(psize), reinterpret_cast<u64*>(d_pivot));
+}
+
+}  // namespace
+
+size_t kway_merge_temp_bytes(int dtype, int k, size_t total) {
+  size_t bytes = 0;
+  if (k < 1) k = 1;
+  dispatch_dtype(dtype, [&](auto tr) { bytes = kway_layout<decltype(tr)>(k, total).total; });
+  return bytes;
+}
+
+cudaError_t kway_merge(int dtype, const void* const* runs, const size_t* lens, int k, void* out, void* d_temp,
+                       size_t temp_bytes, cudaStream_t stream, LaunchRecorder* rec) {
+  cudaError_t result = cudaErrorInvalidValue;
+  dispatch_dtype(dtype, [&](auto tr) {
+    result = kway_merge_typed<decltype(tr)>(runs, lens, k, out, d_temp, temp_bytes, stream, rec);
+  });
+  return result;
+}
+
+cudaError_t pivot_search(int dtype, const void* const* left, const void* const* right, int half, size_t psize,
+                         uint64_t* d_pivot, cudaStream_t stream, LaunchRecorder* rec) {
+  cudaError_t result = cudaErrorInvalidValue;
+  dispatch_dtype(dtype, [&](auto tr) {
+    result = pivot_search_typed<decltype(tr)>(left, right, half, psize, d_pivot, stream, rec);
+  });
+  return result;
+}
+
+}  // namespace mgs

@@ -21,6 +21,7 @@
 //                        into the caller's buffer; reports device status words.
 // Algorithmic HBM traffic: n*w*(2P+1) bytes (+ n*w*2 for an odd pass count).
 #include <algorithm>
+#include <cstdlib>
 #include <mutex>
 
 #include "device_common.cuh"
@@ -178,6 +179,7 @@ struct OnesweepSmem {
   static constexpr int kWarps = BLOCK / 32;
   typename Tr::Bits keys[kTile];  // staged tile, then the tile in digit order
   uint32_t whist[kWarps * kRadix];  // per-warp digit counters -> per-warp offsets
+  uint32_t masks[kWarps * 2 * kRadix];  // per-warp peer masks (shared-memory multisplit)
   uint32_t tile_start[kRadix];      // exclusive scan of the tile's digit counts
   uint32_t gbase[kRadix];           // global scatter base per digit
   uint32_t scan_tmp[kWarps + 1];
@@ -185,13 +187,18 @@ struct OnesweepSmem {
   alignas(8) uint64_t bar;
 };
 
-// Peer mask of lanes holding the same digit. MATCH=0 uses match.any, MATCH=1
-// builds it from 8 ballots (one per digit bit); `ok` separates padding lanes.
+// Peer mask of lanes holding the same digit (the warp multisplit step).
+//   MATCH 0: match.any (one instruction, but it issues many XU-pipe operations)
+//   MATCH 1: 8 ballots, one per digit bit (integer-ALU work)
+//   MATCH 2: per-warp shared-memory masks: every lane ORs its bit into the
+//            mask of its digit, reads the mask back, and the last lane of each
+//            group clears it (masks alternate between two arrays per item).
+// `ok` separates padding lanes of a partial tile (their digit is 256 + lane).
 template <int MATCH, bool FULL>
-__device__ __forceinline__ uint32_t digit_peers(uint32_t d, bool ok) {
+__device__ __forceinline__ uint32_t digit_peers(uint32_t d, bool ok, uint32_t* mm, int lane) {
   if (MATCH == 0) {
     return __match_any_sync(0xffffffffu, d);
-  } else {
+  } else if (MATCH == 1) {
     uint32_t peers = 0xffffffffu;
 #pragma unroll
     for (int b = 0; b < 8; ++b) {
@@ -203,6 +210,11 @@ __device__ __forceinline__ uint32_t digit_peers(uint32_t d, bool ok) {
       const uint32_t bal = __ballot_sync(0xffffffffu, ok);
       peers &= ok ? bal : ~bal;
     }
+    return peers;
+  } else {
+    if (ok) atomicOr(&mm[d], 1u << lane);
+    __syncwarp();
+    const uint32_t peers = ok ? mm[d] : (1u << lane);
     return peers;
   }
 }
@@ -226,17 +238,24 @@ __device__ __forceinline__ void onesweep_tile(OnesweepSmem<Tr, BLOCK, ITEMS>& sm
   Bits key[ITEMS];
   uint32_t rank[ITEMS];
   const int wbase = warp * 32 * ITEMS;
+  const uint32_t lmask_gt = lanemask_gt();
+  uint32_t* mm = sm.masks + warp * 2 * kRadix;
 #pragma unroll
   for (int i = 0; i < ITEMS; ++i) {
     const uint32_t idx = wbase + i * 32 + lane;
     const bool ok = FULL || idx < valid;
     key[i] = sm.keys[idx];
     const uint32_t d = ok ? Tr::Digit(key[i], pass) : (256u + lane);
-    const uint32_t peers = digit_peers<MATCH, FULL>(d, ok);
+    uint32_t* mmi = mm + (i & 1) * kRadix;
+    const uint32_t peers = digit_peers<MATCH, FULL>(d, ok, mmi, lane);
     const uint32_t before = __popc(peers & lmask);
     const uint32_t cnt = ok ? wh[d] : 0u;
     __syncwarp();
-    if (ok && before == 0) wh[d] = cnt + __popc(peers);
+    // the last lane of each peer group advances the warp's digit counter
+    if (ok && (peers & lmask_gt) == 0) {
+      wh[d] = cnt + before + 1u;
+      if (MATCH == 2) mmi[d] = 0u;
+    }
     __syncwarp();
     rank[i] = cnt + before;
   }
@@ -351,6 +370,8 @@ __global__ __launch_bounds__(BLOCK) void radix_onesweep_kernel(typename Tr::Bits
     }
   }
   for (int i = tid; i < kWarps * kRadix; i += BLOCK) sm.whist[i] = 0u;
+  if (MATCH == 2)
+    for (int i = tid; i < kWarps * 2 * kRadix; i += BLOCK) sm.masks[i] = 0u;
   __syncthreads();
   const uint32_t tile = sm.tile_id;
   const size_t base = size_t(tile) * kTile;
@@ -423,6 +444,16 @@ RadixLayout radix_layout(size_t n) {
   return L;
 }
 
+// Warp multisplit strategy of the onesweep ranking (see digit_peers); the
+// MGS_RANK_MODE environment variable selects one for measurements.
+int rank_mode() {
+  static int mode = [] {
+    const char* e = getenv("MGS_RANK_MODE");
+    return (e && (e[0] == '0' || e[0] == '2')) ? e[0] - '0' : 1;
+  }();
+  return mode;
+}
+
 int device_sm_count() {
   int dev = 0, sms = 148;
   if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -478,10 +509,13 @@ cudaError_t radix_sort_typed(typename Tr::Bits* keys, size_t n, void* temp, size
   if (e != cudaSuccess) return e;
 
   const bool use_tma = (reinterpret_cast<uintptr_t>(keys) & 15u) == 0;
+  const int mode = rank_mode();
   if (L.status_bytes == 4) {
-    e = launch_onesweep_passes<Tr, uint32_t, 0>(keys, tmp, st, tb, L, n32, use_tma, stream, rec);
+    if (mode == 0) e = launch_onesweep_passes<Tr, uint32_t, 0>(keys, tmp, st, tb, L, n32, use_tma, stream, rec);
+    else if (mode == 2) e = launch_onesweep_passes<Tr, uint32_t, 2>(keys, tmp, st, tb, L, n32, use_tma, stream, rec);
+    else e = launch_onesweep_passes<Tr, uint32_t, 1>(keys, tmp, st, tb, L, n32, use_tma, stream, rec);
   } else {
-    e = launch_onesweep_passes<Tr, unsigned long long, 0>(keys, tmp, st, tb, L, n32, use_tma, stream, rec);
+    e = launch_onesweep_passes<Tr, unsigned long long, 1>(keys, tmp, st, tb, L, n32, use_tma, stream, rec);
   }
   if (e != cudaSuccess) return e;
 

@@ -83,6 +83,14 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "mgs_sort_device": ([c_void, c_int, c_void, c_size, c_void, c_size, c_void], c_int),
         "mgs_sort_host": ([c_void, c_int, c_void, c_size], c_int),
         "mgs_generate": ([c_int, ctypes.c_char_p, c_u32, c_void, c_size], c_int),
+        "mgs_tanasic_sort": ([c_void, c_int, c_void, c_size, c_int], c_int),
+        "mgs_tanasic_sort_device": ([c_void, c_int, c_void, c_size, c_int], c_int),
+        "mgs_find_pivot_device": ([c_void, c_int, ctypes.POINTER(c_void), ctypes.POINTER(c_void), c_int, c_size,
+                                   ctypes.POINTER(c_size)], c_int),
+        "mgs_merge_temp_bytes": ([c_int, c_int, c_size, ctypes.POINTER(c_size)], c_int),
+        "mgs_merge_device": ([c_void, c_int, c_void, c_size, c_void, c_size, c_void, c_void, c_size, c_void], c_int),
+        "mgs_kway_merge_device": ([c_void, c_int, ctypes.POINTER(c_void), ctypes.POINTER(c_size), c_int, c_void,
+                                   c_void, c_size, c_void], c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -195,6 +203,49 @@ class Context:
         assert keys.flags.c_contiguous
         _check(self._lib.mgs_sort_host(self.handle, dtype_code(keys.dtype), keys.ctypes.data_as(ctypes.c_void_p),
                                        keys.size))
+
+    # --- TanasicSort with g partitions as chunks of this GPU ---
+    def tanasic_sort(self, keys: np.ndarray, num_chunks: int = 1) -> None:
+        """TanasicSort<T>(&keys, gpus) with len(gpus) == num_chunks (src/tanasic_sort.cuh:223-299)."""
+        assert keys.flags.c_contiguous
+        _check(self._lib.mgs_tanasic_sort(self.handle, dtype_code(keys.dtype), keys.ctypes.data_as(ctypes.c_void_p),
+                                          keys.size, int(num_chunks)))
+
+    def tanasic_sort_device(self, d_keys: int, n: int, dtype, num_chunks: int) -> None:
+        _check(self._lib.mgs_tanasic_sort_device(self.handle, dtype_code(dtype), ctypes.c_void_p(d_keys), int(n),
+                                                 int(num_chunks)))
+
+    def find_pivot_device(self, left: list, right: list, chunk_size: int, dtype) -> int:
+        half = len(left)
+        lp = (ctypes.c_void_p * half)(*left)
+        rp = (ctypes.c_void_p * half)(*right)
+        out = ctypes.c_size_t()
+        _check(self._lib.mgs_find_pivot_device(self.handle, dtype_code(dtype), lp, rp, half, int(chunk_size),
+                                               ctypes.byref(out)))
+        return out.value
+
+    @staticmethod
+    def merge_temp_bytes(dtype, k: int, total: int) -> int:
+        lib = load_library()
+        b = ctypes.c_size_t()
+        _check(lib.mgs_merge_temp_bytes(dtype_code(dtype), int(k), int(total), ctypes.byref(b)))
+        return b.value
+
+    def merge_device(self, d_a: int, na: int, d_b: int, nb: int, d_out: int, dtype, d_temp: int = 0,
+                     temp_bytes: int = 0, stream: int = 0) -> None:
+        _check(self._lib.mgs_merge_device(self.handle, dtype_code(dtype), ctypes.c_void_p(d_a), int(na),
+                                          ctypes.c_void_p(d_b), int(nb), ctypes.c_void_p(d_out),
+                                          ctypes.c_void_p(d_temp or None), int(temp_bytes),
+                                          ctypes.c_void_p(stream or None)))
+
+    def kway_merge_device(self, d_runs: list, lens: list, d_out: int, dtype, d_temp: int = 0, temp_bytes: int = 0,
+                          stream: int = 0) -> None:
+        k = len(d_runs)
+        rp = (ctypes.c_void_p * k)(*[p or None for p in d_runs])
+        lp = (ctypes.c_size_t * k)(*[int(x) for x in lens])
+        _check(self._lib.mgs_kway_merge_device(self.handle, dtype_code(dtype), rp, lp, k, ctypes.c_void_p(d_out),
+                                               ctypes.c_void_p(d_temp or None), int(temp_bytes),
+                                               ctypes.c_void_p(stream or None)))
 
     def synchronize(self) -> None:
         _check(self._lib.mgs_ctx_synchronize(self.handle))
