@@ -48,12 +48,12 @@ template <int KEY_BYTES>
 struct OnesweepShape;
 template <>
 struct OnesweepShape<4> {
-  static constexpr int kBlock = 256;
+  static constexpr int kBlock = 512;
   static constexpr int kItems = 16;
 };
 template <>
 struct OnesweepShape<8> {
-  static constexpr int kBlock = 256;
+  static constexpr int kBlock = 512;
   static constexpr int kItems = 8;
 };
 
@@ -62,6 +62,7 @@ constexpr int kHistSub = 4;
 constexpr int kHistUnroll = 4;
 constexpr uint32_t kLookbackSpinLimit = 1u << 25;
 constexpr uint32_t kTmaWaitLimit = 1u << 24;
+constexpr int kLookahead = 8;  // predecessor statuses fetched per look-back round
 
 // Look-back status word: 0 = not published yet; (count + 1) with the top bit
 // clear = this tile's own digit count (aggregate); top bit set = inclusive
@@ -177,14 +178,14 @@ template <class Tr, int BLOCK, int ITEMS>
 struct OnesweepSmem {
   static constexpr int kTile = BLOCK * ITEMS;
   static constexpr int kWarps = BLOCK / 32;
-  typename Tr::Bits keys[kTile];  // staged tile, then the tile in digit order
-  uint32_t whist[kWarps * kRadix];  // per-warp digit counters -> per-warp offsets
+  typename Tr::Bits keys[2][kTile];  // double buffer: tile being sorted / next tile in flight
+  uint32_t whist[kWarps * kRadix];      // per-warp digit counters -> per-warp offsets
   uint32_t masks[kWarps * 2 * kRadix];  // per-warp peer masks (shared-memory multisplit)
-  uint32_t tile_start[kRadix];      // exclusive scan of the tile's digit counts
-  uint32_t gbase[kRadix];           // global scatter base per digit
+  uint32_t tile_start[kRadix];          // exclusive scan of the tile's digit counts
+  uint32_t gbase[kRadix];               // global scatter base per digit
   uint32_t scan_tmp[kWarps + 1];
-  uint32_t tile_id;
-  alignas(8) uint64_t bar;
+  uint32_t tile_id[2];
+  alignas(8) uint64_t bar[2];
 };
 
 // Peer mask of lanes holding the same digit (the warp multisplit step).
@@ -220,99 +221,113 @@ __device__ __forceinline__ uint32_t digit_peers(uint32_t d, bool ok, uint32_t* m
 }
 
 template <class Tr, int BLOCK, int ITEMS, typename StatusT, int MATCH, bool FULL>
-__device__ __forceinline__ void onesweep_tile(OnesweepSmem<Tr, BLOCK, ITEMS>& sm, RadixState* __restrict__ st,
-                                              StatusT* __restrict__ lb_cur, typename Tr::Bits* __restrict__ dst,
-                                              uint32_t tile, uint32_t valid, uint32_t n, int pass) {
+__device__ __forceinline__ void onesweep_tile(OnesweepSmem<Tr, BLOCK, ITEMS>& sm, typename Tr::Bits* skeys,
+                                              RadixState* __restrict__ st, StatusT* __restrict__ lb_cur,
+                                              typename Tr::Bits* __restrict__ dst, uint32_t tile, uint32_t valid,
+                                              uint32_t n, int pass) {
   using Bits = typename Tr::Bits;
   using LW = LookbackWord<StatusT>;
   constexpr int kTile = BLOCK * ITEMS;
   constexpr int kWarps = BLOCK / 32;
   const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
-  uint32_t* wh = sm.whist + warp * kRadix;
-  const uint32_t lmask = lanemask_lt();
-
-  // Rank each key among the keys of its warp with the same digit. Warp w owns
-  // tile positions [w*32*ITEMS, (w+1)*32*ITEMS), item i of lane l is position
-  // w*32*ITEMS + i*32 + l, so ranks follow input order (stability).
-  Bits key[ITEMS];
-  uint32_t rank[ITEMS];
+  uint32_t* wc = sm.whist + warp * kRadix;
   const int wbase = warp * 32 * ITEMS;
+
+  // Phase 1: per-warp digit counts. Warp w owns tile positions
+  // [w*32*ITEMS, (w+1)*32*ITEMS); item i of lane l is position
+  // w*32*ITEMS + i*32 + l, so (warp, item, lane) order is input order.
+  Bits key[ITEMS];
+#pragma unroll
+  for (int i = 0; i < ITEMS; ++i) {
+    const uint32_t idx = wbase + i * 32 + lane;
+    key[i] = skeys[idx];
+    if (FULL || idx < valid) atomicAdd(&wc[Tr::Digit(key[i], pass)], 1u);
+  }
+  __syncthreads();
+
+  // Per digit: publish the tile's count for the look-back right away, then seed
+  // every warp's counter with the position of its first key of that digit.
+  uint32_t tile_count = 0;
+  if (tid < kRadix) {
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) tile_count += sm.whist[w * kRadix + tid];
+    StatusT* slot = lb_cur + size_t(tile) * kRadix + tid;
+    LW::store(slot, tile == 0 ? (LW::kPrefix | StatusT(tile_count)) : StatusT(tile_count + 1u));
+  }
+  uint32_t total;
+  const uint32_t tstart = block_exclusive_scan<BLOCK>(tid < kRadix ? tile_count : 0u, sm.scan_tmp, &total);
+  if (tid < kRadix) {
+    sm.tile_start[tid] = tstart;
+    uint32_t run = tstart;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) {
+      const uint32_t c = sm.whist[w * kRadix + tid];
+      sm.whist[w * kRadix + tid] = run;
+      run += c;
+    }
+  }
+  __syncthreads();
+
+  // Phase 2: stable rank within the warp (peer groups of equal digit, in lane
+  // order) and write each key to its slot of the tile in digit order.
+  const uint32_t lmask = lanemask_lt();
   const uint32_t lmask_gt = lanemask_gt();
   uint32_t* mm = sm.masks + warp * 2 * kRadix;
 #pragma unroll
   for (int i = 0; i < ITEMS; ++i) {
     const uint32_t idx = wbase + i * 32 + lane;
     const bool ok = FULL || idx < valid;
-    key[i] = sm.keys[idx];
     const uint32_t d = ok ? Tr::Digit(key[i], pass) : (256u + lane);
     uint32_t* mmi = mm + (i & 1) * kRadix;
     const uint32_t peers = digit_peers<MATCH, FULL>(d, ok, mmi, lane);
     const uint32_t before = __popc(peers & lmask);
-    const uint32_t cnt = ok ? wh[d] : 0u;
+    const uint32_t pos = ok ? wc[d] + before : 0u;
     __syncwarp();
-    // the last lane of each peer group advances the warp's digit counter
     if (ok && (peers & lmask_gt) == 0) {
-      wh[d] = cnt + before + 1u;
+      wc[d] = pos + 1u;  // the last lane of each peer group advances the counter
       if (MATCH == 2) mmi[d] = 0u;
     }
     __syncwarp();
-    rank[i] = cnt + before;
-  }
-  __syncthreads();
-
-  // Per digit: turn the warp counters into exclusive per-warp offsets, publish
-  // the tile's count for the look-back, and scan the counts across digits.
-  uint32_t tile_count = 0;
-  if (tid < kRadix) {
-#pragma unroll
-    for (int w = 0; w < kWarps; ++w) {
-      const uint32_t t = sm.whist[w * kRadix + tid];
-      sm.whist[w * kRadix + tid] = tile_count;
-      tile_count += t;
-    }
-    StatusT* slot = lb_cur + size_t(tile) * kRadix + tid;
-    LW::store(slot, tile == 0 ? (LW::kPrefix | StatusT(tile_count)) : StatusT(tile_count + 1u));
-  }
-  uint32_t total;
-  const uint32_t tstart = block_exclusive_scan<BLOCK>(tid < kRadix ? tile_count : 0u, sm.scan_tmp, &total);
-  if (tid < kRadix) sm.tile_start[tid] = tstart;
-  __syncthreads();
-
-  // Stage the tile in digit order in shared memory.
-#pragma unroll
-  for (int i = 0; i < ITEMS; ++i) {
-    const uint32_t idx = wbase + i * 32 + lane;
-    if (FULL || idx < valid) {
-      const uint32_t d = Tr::Digit(key[i], pass);
-      const uint32_t pos = sm.tile_start[d] + wh[d] + rank[i];
-      if (pos < uint32_t(kTile)) sm.keys[pos] = key[i];
-    }
+    if (ok && pos < uint32_t(kTile)) skeys[pos] = key[i];
   }
 
   // Decoupled look-back: one thread per digit walks back over earlier tiles,
-  // summing their aggregates until it meets an inclusive prefix.
+  // summing their aggregates until it meets an inclusive prefix. Statuses of
+  // kLookahead predecessors are fetched per round (independent loads).
   if (tid < kRadix) {
     StatusT excl = 0;
     if (tile > 0) {
       long long j = static_cast<long long>(tile) - 1;
       uint32_t spins = 0;
-      while (j >= 0) {
-        const StatusT s = LW::load(lb_cur + size_t(j) * kRadix + tid);
-        if (s == 0) {
+      bool done = false;
+      while (!done && j >= 0) {
+        StatusT sv[kLookahead];
+#pragma unroll
+        for (int q = 0; q < kLookahead; ++q)
+          sv[q] = (j - q >= 0) ? LW::load(lb_cur + size_t(j - q) * kRadix + tid) : (LW::kPrefix | StatusT(0));
+        int used = 0;
+#pragma unroll
+        for (int q = 0; q < kLookahead; ++q) {
+          if (done || used != q) continue;
+          const StatusT v = sv[q];
+          if (v == 0) continue;  // not published yet: poll it again
+          if (v & LW::kPrefix) {
+            excl += v & ~LW::kPrefix;
+            done = true;
+          } else {
+            excl += v - 1;
+            ++used;
+          }
+        }
+        j -= used;
+        if (!done && used == 0) {
           if (++spins >= kLookbackSpinLimit) {
             atomicOr(&st->error, kStatusLookbackTimeout);
             break;
           }
-          if (spins > 16) __nanosleep(32);
-          continue;
+          if (spins > 8) __nanosleep(32);
         }
-        if (s & LW::kPrefix) {
-          excl += s & ~LW::kPrefix;
-          break;
-        }
-        excl += s - 1;
-        --j;
       }
       LW::store(lb_cur + size_t(tile) * kRadix + tid, LW::kPrefix | (excl + tile_count));
     }
@@ -320,76 +335,102 @@ __device__ __forceinline__ void onesweep_tile(OnesweepSmem<Tr, BLOCK, ITEMS>& sm
   }
   __syncthreads();
 
-  // Scatter: consecutive threads write consecutive positions of one digit run.
+  // Phase 3: consecutive threads write consecutive positions of one digit run.
   // The bound check only fails after a look-back timeout (status already set).
 #pragma unroll
   for (int i = 0; i < ITEMS; ++i) {
     const uint32_t idx = i * BLOCK + tid;
     if (FULL || idx < valid) {
-      const Bits k = sm.keys[idx];
+      const Bits k = skeys[idx];
       const uint32_t d = Tr::Digit(k, pass);
-      const uint32_t pos = sm.gbase[d] + idx;
-      if (pos < n) dst[pos] = k;
+      const uint32_t gpos = sm.gbase[d] + idx;
+      if (gpos < n) dst[gpos] = k;
     }
   }
 }
 
 template <class Tr, int BLOCK, int ITEMS, typename StatusT, int MATCH>
-__global__ __launch_bounds__(BLOCK) void radix_onesweep_kernel(typename Tr::Bits* buf0, typename Tr::Bits* buf1,
-                                                               RadixState* __restrict__ st,
-                                                               StatusT* __restrict__ lb_cur,
-                                                               StatusT* __restrict__ lb_next, uint32_t n, int pass,
-                                                               int use_tma) {
+__global__ __launch_bounds__(BLOCK, 1) void radix_onesweep_kernel(typename Tr::Bits* buf0, typename Tr::Bits* buf1,
+                                                                  RadixState* __restrict__ st,
+                                                                  StatusT* __restrict__ lb_cur,
+                                                                  StatusT* __restrict__ lb_next, uint32_t n,
+                                                                  uint32_t num_tiles, int pass, int use_tma) {
   using Bits = typename Tr::Bits;
   using Smem = OnesweepSmem<Tr, BLOCK, ITEMS>;
   constexpr int kTile = Smem::kTile;
   constexpr int kWarps = Smem::kWarps;
+  constexpr uint32_t kTileBytes = uint32_t(kTile * sizeof(Bits));
   static_assert(BLOCK >= kRadix, "one thread per digit");
   extern __shared__ __align__(128) unsigned char smem_raw[];
   Smem& sm = *reinterpret_cast<Smem*>(smem_raw);
   const int tid = threadIdx.x;
 
-  // The next pass uses the other look-back array; this CTA clears its slots.
-  if (lb_next != nullptr && tid < kRadix) lb_next[size_t(blockIdx.x) * kRadix + tid] = 0;
-
+  // The next pass uses the other look-back array; clear it (grid-stride).
+  if (lb_next != nullptr) {
+    const size_t words = size_t(num_tiles) * kRadix;
+    for (size_t i = size_t(blockIdx.x) * BLOCK + tid; i < words; i += size_t(gridDim.x) * BLOCK) lb_next[i] = 0;
+  }
   if (st->skip[pass]) return;  // one digit for every key: identity permutation
   int sel = 0;
   for (int q = 0; q < pass; ++q) sel ^= (st->skip[q] == 0u) ? 1 : 0;
   const Bits* src = sel ? buf1 : buf0;
   Bits* dst = sel ? buf0 : buf1;
 
-  if (tid == 0) {
-    const uint32_t t = atomicAdd(&st->tile_counter[pass], 1u);
-    sm.tile_id = t;
-    const size_t base = size_t(t) * kTile;
-    if (use_tma && base + kTile <= n) {
-      mbar_init(&sm.bar, 1);
-      fence_mbar_init();
-      mbar_arrive_expect_tx(&sm.bar, uint32_t(kTile * sizeof(Bits)));
-      bulk_copy_g2s(sm.keys, src + base, uint32_t(kTile * sizeof(Bits)), &sm.bar);
-    }
-  }
-  for (int i = tid; i < kWarps * kRadix; i += BLOCK) sm.whist[i] = 0u;
+  // Persistent CTA: tiles come in launch order from an atomic counter; the
+  // next tile is claimed and its TMA bulk copy issued before the current tile
+  // is ranked, so loads overlap compute. A CTA's current tile is always older
+  // than its prefetched one, so the oldest unfinished tile is always being
+  // processed and the look-back makes progress.
   if (MATCH == 2)
     for (int i = tid; i < kWarps * 2 * kRadix; i += BLOCK) sm.masks[i] = 0u;
-  __syncthreads();
-  const uint32_t tile = sm.tile_id;
-  const size_t base = size_t(tile) * kTile;
-  const uint32_t valid = uint32_t(min(size_t(kTile), size_t(n) - base));
-  if (use_tma && valid == uint32_t(kTile)) {
-    const bool arrived = mbar_wait_bounded(&sm.bar, 0, kTmaWaitLimit);
-    if (__syncthreads_or(!arrived)) {  // block-uniform exit when the copy never completed
-      if (tid == 0) atomicOr(&st->error, kStatusTmaTimeout);
-      return;
+  if (tid == 0) {
+    mbar_init(&sm.bar[0], 1);
+    mbar_init(&sm.bar[1], 1);
+    fence_mbar_init();
+    const uint32_t t = atomicAdd(&st->tile_counter[pass], 1u);
+    sm.tile_id[0] = t;
+    if (use_tma && t < num_tiles && size_t(t + 1) * kTile <= n) {
+      mbar_arrive_expect_tx(&sm.bar[0], kTileBytes);
+      bulk_copy_g2s(sm.keys[0], src + size_t(t) * kTile, kTileBytes, &sm.bar[0]);
     }
-  } else {
-    for (uint32_t i = tid; i < valid; i += BLOCK) sm.keys[i] = src[base + i];
-    __syncthreads();
   }
-  if (valid == uint32_t(kTile)) {
-    onesweep_tile<Tr, BLOCK, ITEMS, StatusT, MATCH, true>(sm, st, lb_cur, dst, tile, valid, n, pass);
-  } else {
-    onesweep_tile<Tr, BLOCK, ITEMS, StatusT, MATCH, false>(sm, st, lb_cur, dst, tile, valid, n, pass);
+  __syncthreads();
+  uint32_t parity = 0;  // bit b = phase parity of bar[b]
+  int cur = 0;
+  for (;;) {
+    const uint32_t tile = sm.tile_id[cur];
+    if (tile >= num_tiles) break;
+    if (tid == 0) {
+      const uint32_t t = atomicAdd(&st->tile_counter[pass], 1u);
+      sm.tile_id[cur ^ 1] = t;
+      if (use_tma && t < num_tiles && size_t(t + 1) * kTile <= n) {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mbar_arrive_expect_tx(&sm.bar[cur ^ 1], kTileBytes);
+        bulk_copy_g2s(sm.keys[cur ^ 1], src + size_t(t) * kTile, kTileBytes, &sm.bar[cur ^ 1]);
+      }
+    }
+    for (int i = tid; i < kWarps * kRadix; i += BLOCK) sm.whist[i] = 0u;
+    Bits* skeys = sm.keys[cur];
+    const size_t base = size_t(tile) * kTile;
+    const uint32_t valid = uint32_t(min(size_t(kTile), size_t(n) - base));
+    if (use_tma && valid == uint32_t(kTile)) {
+      const bool arrived = mbar_wait_bounded(&sm.bar[cur], (parity >> cur) & 1u, kTmaWaitLimit);
+      parity ^= 1u << cur;
+      if (__syncthreads_or(!arrived)) {  // block-uniform exit when the copy never completed
+        if (tid == 0) atomicOr(&st->error, kStatusTmaTimeout);
+        return;
+      }
+    } else {
+      for (uint32_t i = tid; i < valid; i += BLOCK) skeys[i] = src[base + i];
+      __syncthreads();
+    }
+    if (valid == uint32_t(kTile)) {
+      onesweep_tile<Tr, BLOCK, ITEMS, StatusT, MATCH, true>(sm, skeys, st, lb_cur, dst, tile, valid, n, pass);
+    } else {
+      onesweep_tile<Tr, BLOCK, ITEMS, StatusT, MATCH, false>(sm, skeys, st, lb_cur, dst, tile, valid, n, pass);
+    }
+    __syncthreads();
+    cur ^= 1;
   }
 }
 
@@ -449,7 +490,7 @@ RadixLayout radix_layout(size_t n) {
 int rank_mode() {
   static int mode = [] {
     const char* e = getenv("MGS_RANK_MODE");
-    return (e && (e[0] == '0' || e[0] == '2')) ? e[0] - '0' : 1;
+    return (e && (e[0] == '0' || e[0] == '1')) ? e[0] - '0' : 2;
   }();
   return mode;
 }
@@ -468,15 +509,22 @@ cudaError_t launch_onesweep_passes(typename Tr::Bits* keys, typename Tr::Bits* t
   using Smem = OnesweepSmem<Tr, Shape::kBlock, Shape::kItems>;
   auto kernel = radix_onesweep_kernel<Tr, Shape::kBlock, Shape::kItems, StatusT, MATCH>;
   static std::once_flag once;
+  static int ctas_per_sm = 1;
   std::call_once(once, [&] {
     cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(Smem)));
+    int occ = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, Shape::kBlock, sizeof(Smem)) == cudaSuccess &&
+        occ > 0)
+      ctas_per_sm = occ;
   });
+  const size_t grid = std::min<size_t>(L.num_tiles, size_t(device_sm_count()) * ctas_per_sm);
   StatusT* lb[2] = {reinterpret_cast<StatusT*>(tbase + L.lb0_off), reinterpret_cast<StatusT*>(tbase + L.lb1_off)};
   for (int p = 0; p < Tr::kPasses; ++p) {
     StatusT* cur = lb[p & 1];
     StatusT* next = (p + 1 < Tr::kPasses) ? lb[(p + 1) & 1] : nullptr;
-    cudaError_t e = launch_kernel(rec, "radix_onesweep", kernel, dim3(unsigned(L.num_tiles)), dim3(Shape::kBlock),
-                                  sizeof(Smem), stream, keys, tmp, st, cur, next, n, p, use_tma ? 1 : 0);
+    cudaError_t e = launch_kernel(rec, "radix_onesweep", kernel, dim3(unsigned(grid)), dim3(Shape::kBlock),
+                                  sizeof(Smem), stream, keys, tmp, st, cur, next, n, uint32_t(L.num_tiles), p,
+                                  use_tma ? 1 : 0);
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
@@ -509,13 +557,13 @@ cudaError_t radix_sort_typed(typename Tr::Bits* keys, size_t n, void* temp, size
   if (e != cudaSuccess) return e;
 
   const bool use_tma = (reinterpret_cast<uintptr_t>(keys) & 15u) == 0;
-  const int mode = rank_mode();
+  const int mode = rank_mode();  // default: shared-memory peer masks
   if (L.status_bytes == 4) {
     if (mode == 0) e = launch_onesweep_passes<Tr, uint32_t, 0>(keys, tmp, st, tb, L, n32, use_tma, stream, rec);
-    else if (mode == 2) e = launch_onesweep_passes<Tr, uint32_t, 2>(keys, tmp, st, tb, L, n32, use_tma, stream, rec);
-    else e = launch_onesweep_passes<Tr, uint32_t, 1>(keys, tmp, st, tb, L, n32, use_tma, stream, rec);
+    else if (mode == 1) e = launch_onesweep_passes<Tr, uint32_t, 1>(keys, tmp, st, tb, L, n32, use_tma, stream, rec);
+    else e = launch_onesweep_passes<Tr, uint32_t, 2>(keys, tmp, st, tb, L, n32, use_tma, stream, rec);
   } else {
-    e = launch_onesweep_passes<Tr, unsigned long long, 1>(keys, tmp, st, tb, L, n32, use_tma, stream, rec);
+    e = launch_onesweep_passes<Tr, unsigned long long, 2>(keys, tmp, st, tb, L, n32, use_tma, stream, rec);
   }
   if (e != cudaSuccess) return e;
 
