@@ -105,6 +105,21 @@ int mgs_sort_temp_bytes(int dtype, size_t n, size_t* bytes);
 int mgs_sort_device(mgs_ctx* ctx, int dtype, void* d_keys, size_t n, void* d_temp, size_t temp_bytes,
                     void* stream);
 
+/* ---- device radix sort without any allocation ------------------------------
+ * No counterpart in the reference. For callers that cannot allocate device
+ * memory (code running while a pool or arena owns the device memory,
+ * allocators and runtimes that must not re-enter cudaMalloc, servers that
+ * forbid allocation after start-up): the same sort as mgs_sort_device, with
+ * its scratch in a fixed 32 MiB area that is part of the library's device
+ * image (held by every GPU that loads the library until exit). No context,
+ * no cudaMalloc/cudaFree. At most 7,890,880 keys of 4 bytes or 3,945,440 keys
+ * of 8 bytes; larger n returns MGS_ERR_INVALID. All calls on a GPU share the
+ * area: calls that overlap on that GPU race, so order them on one stream. The
+ * first call on a device looks up the area's address for that device; make it
+ * before any stream capture. Asynchronous on `stream` (a cudaStream_t, NULL =
+ * the legacy default stream); device-side timeouts are not reported. */
+int mgs_sort_device_noalloc(int dtype, void* d_keys, size_t n, void* stream);
+
 /* ---- TanasicSort with one GPU (src/tanasic_sort.cuh:223-299) ------------
  * h_keys is the caller's host buffer (pinned for full link speed); sorted in
  * place: H2D, device sort, D2H, synchronous. Returns early on n == 0 like the

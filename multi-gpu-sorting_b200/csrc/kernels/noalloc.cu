@@ -1,0 +1,99 @@
+// Device sort for callers that cannot allocate device memory.
+//
+// Some callers of a sort cannot call cudaMalloc: code that runs while a
+// memory pool or arena owns all of the device memory, allocators and
+// runtimes that must not re-enter the CUDA allocator, and hosts that forbid
+// allocation once they start serving. For them, mgs_sort_device_noalloc sorts
+// with a fixed scratch area that is part of this library's device image: a
+// file-scope __device__ array, created when the library's module is loaded on
+// a GPU and held by that GPU until the process exits. The caller passes the
+// keys (in and out); nothing else is allocated.
+//
+// Limits and behaviour:
+//   * Scratch is kNoAllocScratchBytes (32 MiB) per GPU. Sorts whose scratch
+//     need (mgs_sort_temp_bytes) exceeds it are rejected with MGS_ERR_INVALID:
+//     up to 7,890,880 keys of 4 bytes or 3,945,440 keys of 8 bytes.
+//   * Every call on a GPU shares the one array. Calls whose work overlaps on
+//     that GPU (different streams, or several host threads) race on it; order
+//     them on one stream or serialize them.
+//   * The array keeps the last call's contents. Everything the sort needs to
+//     start at zero (digit counts, tile counters, look-back status words) is
+//     cleared by each call on its stream before use.
+//   * The first call on a device resolves the array's device address for that
+//     device (cudaGetSymbolAddress, with that device current) and caches it.
+//     Make that first call before any stream capture on the device.
+//   * Asynchronous on `stream`; device-side wait timeouts are not reported
+//     (there is no context status word), the result is then unspecified.
+#include <cuda_runtime.h>
+
+#include <mutex>
+
+#include "engine_types.h"
+#include "mgs.h"
+#include "radix_sort.cuh"
+
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;
+constexpr int kMaxDevices = 64;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+std::mutex g_mutex;
+void* g_scratch_ptr[kMaxDevices] = {};
+
+// Device address of g_noalloc_scratch on `device` (which is current).
+cudaError_t scratch_address(int device, void** out) {
+  std::lock_guard<std::mutex> lock(g_mutex);
+  if (g_scratch_ptr[device] == nullptr) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return e;
+    g_scratch_ptr[device] = p;
+  }
+  *out = g_scratch_ptr[device];
+  return cudaSuccess;
+}
+
+}  // namespace
+
+namespace mgs {
+void set_last_error(const char* fmt, ...);
+void clear_last_error();
+}  // namespace mgs
+
+extern "C" int mgs_sort_device_noalloc(int dtype, void* d_keys, size_t n, void* stream) {
+  const size_t w = mgs::dtype_bytes(dtype);
+  if (w == 0) {
+    mgs::set_last_error("mgs_sort_device_noalloc: unknown dtype");
+    return MGS_ERR_INVALID;
+  }
+  if (n == 0) return MGS_OK;
+  if (d_keys == nullptr || reinterpret_cast<uintptr_t>(d_keys) % w != 0) {
+    mgs::set_last_error("mgs_sort_device_noalloc: d_keys is null or not key-aligned");
+    return MGS_ERR_INVALID;
+  }
+  const size_t need = n < (size_t(1) << 32) ? mgs::radix_sort_temp_bytes(dtype, n) : ~size_t(0);
+  if (need > kNoAllocScratchBytes) {
+    mgs::set_last_error(
+        "mgs_sort_device_noalloc: %zu keys need %zu bytes of scratch; the static scratch holds %zu bytes "
+        "(at most 7890880 keys of 4 bytes or 3945440 keys of 8 bytes)",
+        n, need, kNoAllocScratchBytes);
+    return MGS_ERR_INVALID;
+  }
+  int device = 0;
+  cudaError_t e = cudaGetDevice(&device);
+  if (e == cudaSuccess && (device < 0 || device >= kMaxDevices)) e = cudaErrorInvalidDevice;
+  void* scratch = nullptr;
+  if (e == cudaSuccess) e = scratch_address(device, &scratch);
+  if (e == cudaSuccess)
+    e = mgs::radix_sort(dtype, d_keys, n, scratch, kNoAllocScratchBytes, static_cast<cudaStream_t>(stream), nullptr,
+                        nullptr);
+  if (e != cudaSuccess) {
+    mgs::set_last_error("mgs_sort_device_noalloc: %s", cudaGetErrorString(e));
+    cudaGetLastError();
+    return MGS_ERR_CUDA;
+  }
+  mgs::clear_last_error();
+  return MGS_OK;
+}

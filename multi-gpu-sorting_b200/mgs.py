@@ -82,6 +82,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "mgs_sort_temp_bytes": ([c_int, c_size, ctypes.POINTER(c_size)], c_int),
         "mgs_sort_device": ([c_void, c_int, c_void, c_size, c_void, c_size, c_void], c_int),
         "mgs_sort_host": ([c_void, c_int, c_void, c_size], c_int),
+        "mgs_sort_device_noalloc": ([c_int, c_void, c_size, c_void], c_int),
         "mgs_generate": ([c_int, ctypes.c_char_p, c_u32, c_void, c_size], c_int),
         "mgs_tanasic_sort": ([c_void, c_int, c_void, c_size, c_int], c_int),
         "mgs_tanasic_sort_device": ([c_void, c_int, c_void, c_size, c_int], c_int),
@@ -151,6 +152,15 @@ def generate(dtype, distribution: str, seed: int, n: int, out: np.ndarray | None
     _check(lib.mgs_generate(dtype_code(dtype), distribution.encode(), int(seed) & 0xFFFFFFFF,
                             out.ctypes.data_as(ctypes.c_void_p), int(n)))
     return out
+
+
+def sort_device_noalloc(d_keys: int, n: int, dtype, stream: int = 0) -> None:
+    """mgs_sort_device_noalloc: the device sort without any allocation (fixed 32 MiB scratch in
+    the library's device image; at most 7,890,880 4-byte or 3,945,440 8-byte keys). For callers
+    that cannot call cudaMalloc. Calls that overlap on one GPU race."""
+    lib = load_library()
+    _check(lib.mgs_sort_device_noalloc(dtype_code(dtype), ctypes.c_void_p(d_keys), int(n),
+                                       ctypes.c_void_p(stream or None)))
 
 
 class DataGenerator:
