@@ -112,8 +112,8 @@ int mgs_sort_device(mgs_ctx* ctx, int dtype, void* d_keys, size_t n, void* d_tem
  * forbid allocation after start-up): the same sort as mgs_sort_device, with
  * its scratch in a fixed 32 MiB area that is part of the library's device
  * image (held by every GPU that loads the library until exit). No context,
- * no cudaMalloc/cudaFree. At most 7,890,880 keys of 4 bytes or 3,945,440 keys
- * of 8 bytes; larger n returns MGS_ERR_INVALID. All calls on a GPU share the
+ * no cudaMalloc/cudaFree. At most 2^22 (4,194,304) keys of 4 bytes or 2^21
+ * (2,097,152) keys of 8 bytes; larger n returns MGS_ERR_INVALID. All calls on a GPU share the
  * area: calls that overlap on that GPU race, so order them on one stream. The
  * first call on a device looks up the area's address for that device; make it
  * before any stream capture. Asynchronous on `stream` (a cudaStream_t, NULL =
@@ -158,6 +158,31 @@ int mgs_merge_device(mgs_ctx* ctx, int dtype, const void* d_a, size_t na, const 
                      void* d_temp, size_t temp_bytes, void* stream);
 int mgs_kway_merge_device(mgs_ctx* ctx, int dtype, const void* const* d_runs, const size_t* lens, int k, void* d_out,
                           void* d_temp, size_t temp_bytes, void* stream);
+
+/* ---- GowanlockSort on one GPU: out-of-core chunk pipeline -------------------
+ * (HET sort, src/gowanlock_sort.cuh:127-483). h_keys (host, pinned for full link
+ * speed) is sorted in place. Phase 1 streams chunks of chunk_size keys through
+ * num_buffers (2 or 3, src/gowanlock_sort.cuh:460-469) device buffers: H2D on
+ * one copy engine, radix sort, D2H on the other, overlapped. Phase 2 merges the
+ * sorted chunks: MGS_MERGE_GPU streams windows of the runs through the GPU k-way
+ * merge; MGS_MERGE_CPU runs the reference's __gnu_parallel::multiway_merge with
+ * std::less<T> (src/gowanlock_sort.cuh:73-74,91-92) on the host cores.
+ * chunk_size 0 = the whole input if it fits in 80% of free device memory, else
+ * the largest chunk that does (the reference's default is n / num_gpus,
+ * src/gowanlock_sort.cuh:402-404). merge_group_size is accepted for API parity
+ * (the reference merges groups of chunks on a CPU thread while sorting,
+ * src/gowanlock_sort.cuh:29-84); here the merge is one k-way pass after all
+ * chunks are sorted. At most 1024 chunks with MGS_MERGE_GPU. A pinned host
+ * buffer of n keys holds the sorted chunks; it is kept by the context
+ * (grow-only). Synchronous. Phase times: mgs_ctx_phase_seconds. */
+#define MGS_MERGE_GPU 0
+#define MGS_MERGE_CPU 1
+int mgs_gowanlock_sort(mgs_ctx* ctx, int dtype, void* h_keys, size_t n, size_t chunk_size, size_t merge_group_size,
+                       size_t num_buffers, int merge_mode);
+/* Wall-clock seconds of the context's last GowanlockSort call per phase, named
+ * like the reference's TimeDurations keys (src/time_durations.cuh): "memory_allocation",
+ * "sort_phase" (chunk sorting and merging), "merge_phase", "memory_deallocation". */
+int mgs_ctx_phase_seconds(mgs_ctx* ctx, const char* phase, double* seconds);
 
 /* ---- DataGenerator::ComputeDistribution<T> (src/data_generator.cuh:18-36) ----
  * Fills the host buffer out[0..n) exactly as the reference generator does for

@@ -5,6 +5,7 @@
 
 #include <cuda_runtime.h>
 
+#include <chrono>
 #include <cstring>
 #include <new>
 #include <string>
@@ -14,6 +15,7 @@
 #include "../kernels/radix_sort.cuh"
 #include "chunk_sort.h"
 #include "context.h"
+#include "out_of_core.h"
 
 namespace mgs {
 bool generate_keys(int dtype, const char* distribution, uint32_t seed, void* out, size_t n);
@@ -132,6 +134,7 @@ int mgs_ctx_destroy(mgs_ctx* ctx) {
     if (c.arena) cudaFree(c.arena);
     if (c.d_status) cudaFree(c.d_status);
     if (c.h_status) cudaFreeHost(c.h_status);
+    if (c.host_arena) cudaFreeHost(c.host_arena);
     if (c.compute) cudaStreamDestroy(c.compute);
     if (c.h2d) cudaStreamDestroy(c.h2d);
     if (c.d2h) cudaStreamDestroy(c.d2h);
@@ -396,6 +399,55 @@ int mgs_merge_device(mgs_ctx* ctx, int dtype, const void* d_a, size_t na, const 
   const void* runs[2] = {d_a, d_b};
   const size_t lens[2] = {na, nb};
   return mgs_kway_merge_device(ctx, dtype, runs, lens, 2, d_out, d_temp, temp_bytes, stream);
+}
+
+int mgs_gowanlock_sort(mgs_ctx* ctx, int dtype, void* h_keys, size_t n, size_t chunk_size, size_t merge_group_size,
+                       size_t num_buffers, int merge_mode) {
+  if (!ctx) return invalid("mgs_gowanlock_sort: ctx is null");
+  const size_t w = mgs::dtype_bytes(dtype);
+  if (w == 0) return invalid("mgs_gowanlock_sort: unknown dtype");
+  if (num_buffers != 2 && num_buffers != 3) return invalid("mgs_gowanlock_sort: num_buffers must be 2 or 3");
+  if (merge_mode != MGS_MERGE_GPU && merge_mode != MGS_MERGE_CPU)
+    return invalid("mgs_gowanlock_sort: merge_mode must be MGS_MERGE_GPU or MGS_MERGE_CPU");
+  (void)merge_group_size;  // 0 = automatic; the merge is one k-way pass (see mgs.h)
+  if (n == 0) return MGS_OK;  // src/gowanlock_sort.cuh:398-400
+  if (!h_keys) return invalid("mgs_gowanlock_sort: h_keys is null");
+  Context& c = ctx->impl;
+  DeviceGuard g(c.device);
+  size_t free_b = 0, total_b = 0;
+  cudaError_t e = cudaMemGetInfo(&free_b, &total_b);
+  if (e != cudaSuccess) return cuda_fail(e, "mgs_gowanlock_sort: cudaMemGetInfo");
+  const size_t budget = (free_b + c.arena_bytes) / 10 * 8;
+  const mgs::OocPlan plan = mgs::plan_out_of_core(dtype, n, chunk_size, int(num_buffers), 0, budget);
+  if (merge_mode == MGS_MERGE_GPU && plan.num_chunks > size_t(mgs::kMaxKwayRuns))
+    return invalid("mgs_gowanlock_sort: more than 1024 chunks; use a larger chunk_size");
+  const auto t0 = std::chrono::steady_clock::now();
+  if (plan.num_chunks > 1) {
+    e = c.reserve_host(n * w);
+    if (e != cudaSuccess) return cuda_fail(e, "mgs_gowanlock_sort: pinned secondary buffer");
+  }
+  const double host_alloc_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  mgs::OocTimes t;
+  e = mgs::out_of_core_sort(c, dtype, h_keys, n, plan, merge_mode == MGS_MERGE_CPU, c.host_arena, &t);
+  if (e != cudaSuccess) return cuda_fail(e, "mgs_gowanlock_sort");
+  c.phase_s[0] = host_alloc_s + t.allocation_s;
+  c.phase_s[1] = t.sort_s + t.merge_s;
+  c.phase_s[2] = t.merge_s;
+  c.phase_s[3] = 0;
+  return finish_sync(c, "mgs_gowanlock_sort: synchronize");
+}
+
+int mgs_ctx_phase_seconds(mgs_ctx* ctx, const char* phase, double* seconds) {
+  if (!ctx || !phase || !seconds) return invalid("mgs_ctx_phase_seconds: null argument");
+  static const char* names[4] = {"memory_allocation", "sort_phase", "merge_phase", "memory_deallocation"};
+  for (int i = 0; i < 4; ++i) {
+    if (std::strcmp(phase, names[i]) == 0) {
+      *seconds = ctx->impl.phase_s[i];
+      return MGS_OK;
+    }
+  }
+  set_last_error("mgs_ctx_phase_seconds: unknown phase '%s'", phase);
+  return MGS_ERR_INVALID;
 }
 
 int mgs_generate(int dtype, const char* distribution, uint32_t seed, void* out, size_t n) {

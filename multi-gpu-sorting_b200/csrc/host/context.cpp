@@ -101,6 +101,21 @@ cudaError_t Context::reserve(size_t bytes) {
   return cudaSuccess;
 }
 
+cudaError_t Context::reserve_host(size_t bytes) {
+  if (bytes <= host_arena_bytes) return cudaSuccess;
+  if (host_arena) cudaFreeHost(host_arena);
+  host_arena = nullptr;
+  host_arena_bytes = 0;
+  cudaError_t e = cudaHostAlloc(&host_arena, bytes, cudaHostAllocDefault);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    host_arena = nullptr;
+    return cudaErrorMemoryAllocation;
+  }
+  host_arena_bytes = bytes;
+  return cudaSuccess;
+}
+
 cudaError_t Context::take_status(cudaStream_t stream, uint32_t* status) {
   cudaError_t e = cudaMemcpyAsync(h_status, d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(stream);

@@ -57,6 +57,12 @@ struct Context {
   uint32_t* h_status = nullptr;  // pinned mirror used by status reads
   uint64_t* h_status64 = nullptr;  // pinned 8-byte word (pivot readback), inside the h_status block
   EventRecorder recorder;
+  void* host_arena = nullptr;  // grow-only pinned host buffer (out-of-core sorted runs)
+  size_t host_arena_bytes = 0;
+  double phase_s[4] = {0, 0, 0, 0};  // last call's memory_allocation, sort_phase, merge_phase, memory_deallocation
+
+  // Ensures the pinned host arena holds at least `bytes`.
+  cudaError_t reserve_host(size_t bytes);
 
   // Ensures the arena holds at least `bytes` (synchronizes before growing).
   cudaError_t reserve(size_t bytes);

@@ -10,9 +10,10 @@
 // keys (in and out); nothing else is allocated.
 //
 // Limits and behaviour:
-//   * Scratch is kNoAllocScratchBytes (32 MiB) per GPU. Sorts whose scratch
-//     need (mgs_sort_temp_bytes) exceeds it are rejected with MGS_ERR_INVALID:
-//     up to 7,890,880 keys of 4 bytes or 3,945,440 keys of 8 bytes.
+//   * Scratch is kNoAllocScratchBytes (32 MiB) per GPU. A call sorts at most
+//     2^22 (4,194,304) keys of 4 bytes or 2^21 (2,097,152) keys of 8 bytes
+//     (their scratch need, mgs_sort_temp_bytes, stays below 20 MiB); larger n is
+//     rejected with MGS_ERR_INVALID.
 //   * Every call on a GPU shares the one array. Calls whose work overlaps on
 //     that GPU (different streams, or several host threads) race on it; order
 //     them on one stream or serialize them.
@@ -35,6 +36,7 @@
 namespace {
 
 constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;
+constexpr size_t kNoAllocMaxBytesOfKeys = size_t(16) << 20;  // 2^22 4-byte keys or 2^21 8-byte keys
 constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
@@ -73,12 +75,11 @@ extern "C" int mgs_sort_device_noalloc(int dtype, void* d_keys, size_t n, void* 
     mgs::set_last_error("mgs_sort_device_noalloc: d_keys is null or not key-aligned");
     return MGS_ERR_INVALID;
   }
-  const size_t need = n < (size_t(1) << 32) ? mgs::radix_sort_temp_bytes(dtype, n) : ~size_t(0);
-  if (need > kNoAllocScratchBytes) {
+  const size_t max_keys = kNoAllocMaxBytesOfKeys / w;
+  if (n > max_keys || mgs::radix_sort_temp_bytes(dtype, n) > kNoAllocScratchBytes) {
     mgs::set_last_error(
-        "mgs_sort_device_noalloc: %zu keys need %zu bytes of scratch; the static scratch holds %zu bytes "
-        "(at most 7890880 keys of 4 bytes or 3945440 keys of 8 bytes)",
-        n, need, kNoAllocScratchBytes);
+        "mgs_sort_device_noalloc: %zu keys exceed the static scratch (%zu bytes): at most %zu keys of %zu bytes", n,
+        kNoAllocScratchBytes, max_keys, w);
     return MGS_ERR_INVALID;
   }
   int device = 0;

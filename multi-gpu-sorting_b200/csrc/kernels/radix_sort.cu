@@ -43,19 +43,33 @@ struct RadixState {
   uint32_t pad[7];
 };
 
-// Tile shape per key width (threads x keys per thread).
-template <int KEY_BYTES>
+// Tile shapes per key width: threads x keys per thread, CTAs per SM, ranking
+// chains per warp. The default (shape 5: 512 threads x 32 keys, 16384-key
+// tiles) is the fastest measured on B200 without register spills.
+template <int KEY_BYTES, int SHAPE>
 struct OnesweepShape;
-template <>
-struct OnesweepShape<4> {
-  static constexpr int kBlock = 512;
-  static constexpr int kItems = 16;
-};
-template <>
-struct OnesweepShape<8> {
-  static constexpr int kBlock = 512;
-  static constexpr int kItems = 8;
-};
+#define MGS_SHAPE(W, S, B, I, M, C)                                                 \
+  template <>                                                                      \
+  struct OnesweepShape<W, S> {                                                     \
+    static constexpr int kBlock = B, kItems = I, kMinBlocks = M, kChains = C;      \
+  };
+MGS_SHAPE(4, 0, 512, 16, 1, 1)
+MGS_SHAPE(4, 1, 256, 16, 2, 1)
+MGS_SHAPE(4, 2, 512, 24, 1, 1)
+MGS_SHAPE(4, 3, 512, 24, 1, 2)
+MGS_SHAPE(4, 4, 512, 32, 1, 2)
+MGS_SHAPE(4, 5, 512, 32, 1, 1)
+MGS_SHAPE(4, 6, 512, 40, 1, 1)
+MGS_SHAPE(8, 0, 512, 8, 1, 1)
+MGS_SHAPE(8, 1, 256, 8, 2, 1)
+MGS_SHAPE(8, 2, 512, 12, 1, 1)
+MGS_SHAPE(8, 3, 512, 12, 1, 2)
+MGS_SHAPE(8, 4, 512, 16, 1, 2)
+MGS_SHAPE(8, 5, 512, 16, 1, 1)
+MGS_SHAPE(8, 6, 512, 20, 1, 1)
+#undef MGS_SHAPE
+constexpr int kNumShapes = 7;
+constexpr int kDefaultShape = 5;
 
 constexpr int kHistBlock = 256;
 constexpr int kHistSub = 4;
@@ -174,15 +188,16 @@ __global__ __launch_bounds__(kRadix) void radix_scan_kernel(RadixState* __restri
 }
 
 // ---------------------------------------------------------------- K2 --------
-template <class Tr, int BLOCK, int ITEMS>
+template <class Tr, int BLOCK, int ITEMS, int CHAINS>
 struct OnesweepSmem {
   static constexpr int kTile = BLOCK * ITEMS;
   static constexpr int kWarps = BLOCK / 32;
-  typename Tr::Bits keys[2][kTile];  // double buffer: tile being sorted / next tile in flight
-  uint32_t whist[kWarps * kRadix];      // per-warp digit counters -> per-warp offsets
-  uint32_t masks[kWarps * 2 * kRadix];  // per-warp peer masks (shared-memory multisplit)
-  uint32_t tile_start[kRadix];          // exclusive scan of the tile's digit counts
-  uint32_t gbase[kRadix];               // global scatter base per digit
+  static constexpr int kChains = kWarps * CHAINS;  // ranking chains (CHAINS per warp)
+  typename Tr::Bits keys[2][kTile];    // double buffer: tile being sorted / next tile in flight
+  uint32_t ccount[kChains * kRadix];     // per-chain digit counters -> tile positions
+  uint32_t masks[kChains * 2 * kRadix];  // per-chain peer masks (shared-memory multisplit)
+  uint32_t tile_start[kRadix];           // exclusive scan of the tile's digit counts
+  uint32_t gbase[kRadix];                // global scatter base per digit
   uint32_t scan_tmp[kWarps + 1];
   uint32_t tile_id[2];
   alignas(8) uint64_t bar[2];
@@ -191,7 +206,7 @@ struct OnesweepSmem {
 // Peer mask of lanes holding the same digit (the warp multisplit step).
 //   MATCH 0: match.any (one instruction, but it issues many XU-pipe operations)
 //   MATCH 1: 8 ballots, one per digit bit (integer-ALU work)
-//   MATCH 2: per-warp shared-memory masks: every lane ORs its bit into the
+//   MATCH 2: per-chain shared-memory masks: every lane ORs its bit into the
 //            mask of its digit, reads the mask back, and the last lane of each
 //            group clears it (masks alternate between two arrays per item).
 // `ok` separates padding lanes of a partial tile (their digit is 256 + lane).
@@ -215,43 +230,49 @@ __device__ __forceinline__ uint32_t digit_peers(uint32_t d, bool ok, uint32_t* m
   } else {
     if (ok) atomicOr(&mm[d], 1u << lane);
     __syncwarp();
-    const uint32_t peers = ok ? mm[d] : (1u << lane);
-    return peers;
+    return ok ? mm[d] : (1u << lane);
   }
 }
 
-template <class Tr, int BLOCK, int ITEMS, typename StatusT, int MATCH, bool FULL>
-__device__ __forceinline__ void onesweep_tile(OnesweepSmem<Tr, BLOCK, ITEMS>& sm, typename Tr::Bits* skeys,
+// One tile: count, publish, rank into shared memory in digit order, look back,
+// scatter. Warp w owns tile positions [w*32*ITEMS, (w+1)*32*ITEMS); item i of
+// lane l is position w*32*ITEMS + i*32 + l, so (warp, item, lane) is input
+// order. With CHAINS = 2 the warp's items split into two halves that are
+// ranked as independent chains (own counters and masks), interleaved so that
+// their shared-memory latencies overlap; the second half's counters start
+// after the first half's keys of the same digit.
+template <class Tr, int BLOCK, int ITEMS, int CHAINS, typename StatusT, int MATCH, bool FULL>
+__device__ __forceinline__ void onesweep_tile(OnesweepSmem<Tr, BLOCK, ITEMS, CHAINS>& sm, typename Tr::Bits* skeys,
                                               RadixState* __restrict__ st, StatusT* __restrict__ lb_cur,
                                               typename Tr::Bits* __restrict__ dst, uint32_t tile, uint32_t valid,
                                               uint32_t n, int pass) {
   using Bits = typename Tr::Bits;
   using LW = LookbackWord<StatusT>;
   constexpr int kTile = BLOCK * ITEMS;
-  constexpr int kWarps = BLOCK / 32;
+  constexpr int kChains = (BLOCK / 32) * CHAINS;
+  constexpr int kPerChain = ITEMS / CHAINS;
+  static_assert(ITEMS % CHAINS == 0, "items split evenly into chains");
   const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
-  uint32_t* wc = sm.whist + warp * kRadix;
   const int wbase = warp * 32 * ITEMS;
 
-  // Phase 1: per-warp digit counts. Warp w owns tile positions
-  // [w*32*ITEMS, (w+1)*32*ITEMS); item i of lane l is position
-  // w*32*ITEMS + i*32 + l, so (warp, item, lane) order is input order.
+  // Phase 1: per-chain digit counts.
   Bits key[ITEMS];
 #pragma unroll
   for (int i = 0; i < ITEMS; ++i) {
     const uint32_t idx = wbase + i * 32 + lane;
     key[i] = skeys[idx];
-    if (FULL || idx < valid) atomicAdd(&wc[Tr::Digit(key[i], pass)], 1u);
+    uint32_t* cc = sm.ccount + (warp * CHAINS + i / kPerChain) * kRadix;
+    if (FULL || idx < valid) atomicAdd(&cc[Tr::Digit(key[i], pass)], 1u);
   }
   __syncthreads();
 
   // Per digit: publish the tile's count for the look-back right away, then seed
-  // every warp's counter with the position of its first key of that digit.
+  // every chain's counter with the tile position of its first key of that digit.
   uint32_t tile_count = 0;
   if (tid < kRadix) {
 #pragma unroll
-    for (int w = 0; w < kWarps; ++w) tile_count += sm.whist[w * kRadix + tid];
+    for (int c = 0; c < kChains; ++c) tile_count += sm.ccount[c * kRadix + tid];
     StatusT* slot = lb_cur + size_t(tile) * kRadix + tid;
     LW::store(slot, tile == 0 ? (LW::kPrefix | StatusT(tile_count)) : StatusT(tile_count + 1u));
   }
@@ -261,35 +282,58 @@ __device__ __forceinline__ void onesweep_tile(OnesweepSmem<Tr, BLOCK, ITEMS>& sm
     sm.tile_start[tid] = tstart;
     uint32_t run = tstart;
 #pragma unroll
-    for (int w = 0; w < kWarps; ++w) {
-      const uint32_t c = sm.whist[w * kRadix + tid];
-      sm.whist[w * kRadix + tid] = run;
-      run += c;
+    for (int c = 0; c < kChains; ++c) {
+      const uint32_t v = sm.ccount[c * kRadix + tid];
+      sm.ccount[c * kRadix + tid] = run;
+      run += v;
     }
   }
   __syncthreads();
 
-  // Phase 2: stable rank within the warp (peer groups of equal digit, in lane
-  // order) and write each key to its slot of the tile in digit order.
+  // Phase 2: stable rank within each chain (peer groups of equal digit, in lane
+  // order); each key goes straight to its slot of the tile in digit order.
   const uint32_t lmask = lanemask_lt();
   const uint32_t lmask_gt = lanemask_gt();
-  uint32_t* mm = sm.masks + warp * 2 * kRadix;
 #pragma unroll
-  for (int i = 0; i < ITEMS; ++i) {
-    const uint32_t idx = wbase + i * 32 + lane;
-    const bool ok = FULL || idx < valid;
-    const uint32_t d = ok ? Tr::Digit(key[i], pass) : (256u + lane);
-    uint32_t* mmi = mm + (i & 1) * kRadix;
-    const uint32_t peers = digit_peers<MATCH, FULL>(d, ok, mmi, lane);
-    const uint32_t before = __popc(peers & lmask);
-    const uint32_t pos = ok ? wc[d] + before : 0u;
+  for (int j = 0; j < kPerChain; ++j) {
+    uint32_t d[CHAINS], peers[CHAINS], pos[CHAINS];
+    bool ok[CHAINS];
+    uint32_t* cc[CHAINS];
+    uint32_t* mm[CHAINS];
+#pragma unroll
+    for (int h = 0; h < CHAINS; ++h) {
+      const int i = h * kPerChain + j;
+      const uint32_t idx = wbase + i * 32 + lane;
+      ok[h] = FULL || idx < valid;
+      d[h] = ok[h] ? Tr::Digit(key[i], pass) : (256u + lane);
+      cc[h] = sm.ccount + (warp * CHAINS + h) * kRadix;
+      mm[h] = sm.masks + (warp * CHAINS + h) * 2 * kRadix + (j & 1) * kRadix;
+    }
+    if (MATCH == 2) {
+#pragma unroll
+      for (int h = 0; h < CHAINS; ++h)
+        if (ok[h]) atomicOr(&mm[h][d[h]], 1u << lane);
+      __syncwarp();
+#pragma unroll
+      for (int h = 0; h < CHAINS; ++h) peers[h] = ok[h] ? mm[h][d[h]] : (1u << lane);
+    } else {
+#pragma unroll
+      for (int h = 0; h < CHAINS; ++h) peers[h] = digit_peers<MATCH, FULL>(d[h], ok[h], mm[h], lane);
+    }
+#pragma unroll
+    for (int h = 0; h < CHAINS; ++h) pos[h] = ok[h] ? cc[h][d[h]] + __popc(peers[h] & lmask) : 0u;
     __syncwarp();
-    if (ok && (peers & lmask_gt) == 0) {
-      wc[d] = pos + 1u;  // the last lane of each peer group advances the counter
-      if (MATCH == 2) mmi[d] = 0u;
+#pragma unroll
+    for (int h = 0; h < CHAINS; ++h) {
+      if (ok[h] && (peers[h] & lmask_gt) == 0) {
+        cc[h][d[h]] = pos[h] + 1u;  // the last lane of each peer group advances the counter
+        if (MATCH == 2) mm[h][d[h]] = 0u;
+      }
     }
     __syncwarp();
-    if (ok && pos < uint32_t(kTile)) skeys[pos] = key[i];
+#pragma unroll
+    for (int h = 0; h < CHAINS; ++h)
+      if (ok[h] && pos[h] < uint32_t(kTile)) skeys[pos[h]] = key[h * kPerChain + j];
   }
 
   // Decoupled look-back: one thread per digit walks back over earlier tiles,
@@ -298,14 +342,14 @@ __device__ __forceinline__ void onesweep_tile(OnesweepSmem<Tr, BLOCK, ITEMS>& sm
   if (tid < kRadix) {
     StatusT excl = 0;
     if (tile > 0) {
-      long long j = static_cast<long long>(tile) - 1;
+      long long jt = static_cast<long long>(tile) - 1;
       uint32_t spins = 0;
       bool done = false;
-      while (!done && j >= 0) {
+      while (!done && jt >= 0) {
         StatusT sv[kLookahead];
 #pragma unroll
         for (int q = 0; q < kLookahead; ++q)
-          sv[q] = (j - q >= 0) ? LW::load(lb_cur + size_t(j - q) * kRadix + tid) : (LW::kPrefix | StatusT(0));
+          sv[q] = (jt - q >= 0) ? LW::load(lb_cur + size_t(jt - q) * kRadix + tid) : (LW::kPrefix | StatusT(0));
         int used = 0;
 #pragma unroll
         for (int q = 0; q < kLookahead; ++q) {
@@ -320,7 +364,7 @@ __device__ __forceinline__ void onesweep_tile(OnesweepSmem<Tr, BLOCK, ITEMS>& sm
             ++used;
           }
         }
-        j -= used;
+        jt -= used;
         if (!done && used == 0) {
           if (++spins >= kLookbackSpinLimit) {
             atomicOr(&st->error, kStatusLookbackTimeout);
@@ -342,23 +386,22 @@ __device__ __forceinline__ void onesweep_tile(OnesweepSmem<Tr, BLOCK, ITEMS>& sm
     const uint32_t idx = i * BLOCK + tid;
     if (FULL || idx < valid) {
       const Bits k = skeys[idx];
-      const uint32_t d = Tr::Digit(k, pass);
-      const uint32_t gpos = sm.gbase[d] + idx;
+      const uint32_t gpos = sm.gbase[Tr::Digit(k, pass)] + idx;
       if (gpos < n) dst[gpos] = k;
     }
   }
 }
 
-template <class Tr, int BLOCK, int ITEMS, typename StatusT, int MATCH>
-__global__ __launch_bounds__(BLOCK, 1) void radix_onesweep_kernel(typename Tr::Bits* buf0, typename Tr::Bits* buf1,
-                                                                  RadixState* __restrict__ st,
-                                                                  StatusT* __restrict__ lb_cur,
-                                                                  StatusT* __restrict__ lb_next, uint32_t n,
-                                                                  uint32_t num_tiles, int pass, int use_tma) {
+template <class Tr, int BLOCK, int ITEMS, int MINB, int CHAINS, typename StatusT, int MATCH>
+__global__ __launch_bounds__(BLOCK, MINB) void radix_onesweep_kernel(typename Tr::Bits* buf0, typename Tr::Bits* buf1,
+                                                                     RadixState* __restrict__ st,
+                                                                     StatusT* __restrict__ lb_cur,
+                                                                     StatusT* __restrict__ lb_next, uint32_t n,
+                                                                     uint32_t num_tiles, int pass, int use_tma) {
   using Bits = typename Tr::Bits;
-  using Smem = OnesweepSmem<Tr, BLOCK, ITEMS>;
+  using Smem = OnesweepSmem<Tr, BLOCK, ITEMS, CHAINS>;
   constexpr int kTile = Smem::kTile;
-  constexpr int kWarps = Smem::kWarps;
+  constexpr int kChains = Smem::kChains;
   constexpr uint32_t kTileBytes = uint32_t(kTile * sizeof(Bits));
   static_assert(BLOCK >= kRadix, "one thread per digit");
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -382,7 +425,7 @@ __global__ __launch_bounds__(BLOCK, 1) void radix_onesweep_kernel(typename Tr::B
   // than its prefetched one, so the oldest unfinished tile is always being
   // processed and the look-back makes progress.
   if (MATCH == 2)
-    for (int i = tid; i < kWarps * 2 * kRadix; i += BLOCK) sm.masks[i] = 0u;
+    for (int i = tid; i < kChains * 2 * kRadix; i += BLOCK) sm.masks[i] = 0u;
   if (tid == 0) {
     mbar_init(&sm.bar[0], 1);
     mbar_init(&sm.bar[1], 1);
@@ -409,7 +452,7 @@ __global__ __launch_bounds__(BLOCK, 1) void radix_onesweep_kernel(typename Tr::B
         bulk_copy_g2s(sm.keys[cur ^ 1], src + size_t(t) * kTile, kTileBytes, &sm.bar[cur ^ 1]);
       }
     }
-    for (int i = tid; i < kWarps * kRadix; i += BLOCK) sm.whist[i] = 0u;
+    for (int i = tid; i < kChains * kRadix; i += BLOCK) sm.ccount[i] = 0u;
     Bits* skeys = sm.keys[cur];
     const size_t base = size_t(tile) * kTile;
     const uint32_t valid = uint32_t(min(size_t(kTile), size_t(n) - base));
@@ -425,9 +468,9 @@ __global__ __launch_bounds__(BLOCK, 1) void radix_onesweep_kernel(typename Tr::B
       __syncthreads();
     }
     if (valid == uint32_t(kTile)) {
-      onesweep_tile<Tr, BLOCK, ITEMS, StatusT, MATCH, true>(sm, skeys, st, lb_cur, dst, tile, valid, n, pass);
+      onesweep_tile<Tr, BLOCK, ITEMS, CHAINS, StatusT, MATCH, true>(sm, skeys, st, lb_cur, dst, tile, valid, n, pass);
     } else {
-      onesweep_tile<Tr, BLOCK, ITEMS, StatusT, MATCH, false>(sm, skeys, st, lb_cur, dst, tile, valid, n, pass);
+      onesweep_tile<Tr, BLOCK, ITEMS, CHAINS, StatusT, MATCH, false>(sm, skeys, st, lb_cur, dst, tile, valid, n, pass);
     }
     __syncthreads();
     cur ^= 1;
@@ -469,14 +512,41 @@ struct RadixLayout {
   size_t num_tiles, status_bytes;
 };
 
+// Onesweep shape and multisplit strategy; the MGS_ONESWEEP_SHAPE and
+// MGS_RANK_MODE environment variables select alternatives for measurements.
+int onesweep_shape() {
+  static int shape = [] {
+    const char* e = getenv("MGS_ONESWEEP_SHAPE");
+    return (e && e[0] >= '0' && e[0] < '0' + kNumShapes) ? e[0] - '0' : kDefaultShape;
+  }();
+  return shape;
+}
+
+int rank_mode() {
+  static int mode = [] {
+    const char* e = getenv("MGS_RANK_MODE");
+    return (e && e[0] >= '0' && e[0] <= '2') ? e[0] - '0' : 2;
+  }();
+  return mode;
+}
+
+template <int KEY_BYTES, int SHAPE>
+constexpr size_t shape_tile() {
+  return size_t(OnesweepShape<KEY_BYTES, SHAPE>::kBlock) * OnesweepShape<KEY_BYTES, SHAPE>::kItems;
+}
+
 template <class Tr>
 RadixLayout radix_layout(size_t n) {
-  using Shape = OnesweepShape<sizeof(typename Tr::Bits)>;
-  constexpr size_t kTile = size_t(Shape::kBlock) * Shape::kItems;
+  constexpr int w = int(sizeof(typename Tr::Bits));
+  constexpr size_t tiles[kNumShapes] = {shape_tile<w, 0>(), shape_tile<w, 1>(), shape_tile<w, 2>(), shape_tile<w, 3>(),
+                                         shape_tile<w, 4>(), shape_tile<w, 5>(), shape_tile<w, 6>()};
+  const size_t tile = tiles[onesweep_shape()];
+  // The look-back arrays are sized for the smallest tile, so every shape fits.
+  constexpr size_t min_tile = shape_tile<w, 1>();
   RadixLayout L;
-  L.num_tiles = (n + kTile - 1) / kTile;
+  L.num_tiles = (n + tile - 1) / tile;
   L.status_bytes = (n < (size_t(1) << 31)) ? 4 : 8;
-  const size_t lb_bytes = L.num_tiles * kRadix * L.status_bytes;
+  const size_t lb_bytes = ((n + min_tile - 1) / min_tile) * kRadix * L.status_bytes;
   L.state_off = 0;
   L.lb0_off = align_up(sizeof(RadixState), 256);
   L.lb1_off = L.lb0_off + align_up(lb_bytes, 256);
@@ -485,29 +555,20 @@ RadixLayout radix_layout(size_t n) {
   return L;
 }
 
-// Warp multisplit strategy of the onesweep ranking (see digit_peers); the
-// MGS_RANK_MODE environment variable selects one for measurements.
-int rank_mode() {
-  static int mode = [] {
-    const char* e = getenv("MGS_RANK_MODE");
-    return (e && (e[0] == '0' || e[0] == '1')) ? e[0] - '0' : 2;
-  }();
-  return mode;
-}
-
 int device_sm_count() {
   int dev = 0, sms = 148;
   if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   return sms > 0 ? sms : 148;
 }
 
-template <class Tr, typename StatusT, int MATCH>
+template <class Tr, int SHAPE, typename StatusT, int MATCH>
 cudaError_t launch_onesweep_passes(typename Tr::Bits* keys, typename Tr::Bits* tmp, RadixState* st, char* tbase,
                                    const RadixLayout& L, uint32_t n, bool use_tma, cudaStream_t stream,
                                    LaunchRecorder* rec) {
-  using Shape = OnesweepShape<sizeof(typename Tr::Bits)>;
-  using Smem = OnesweepSmem<Tr, Shape::kBlock, Shape::kItems>;
-  auto kernel = radix_onesweep_kernel<Tr, Shape::kBlock, Shape::kItems, StatusT, MATCH>;
+  using Shape = OnesweepShape<sizeof(typename Tr::Bits), SHAPE>;
+  using Smem = OnesweepSmem<Tr, Shape::kBlock, Shape::kItems, Shape::kChains>;
+  auto kernel =
+      radix_onesweep_kernel<Tr, Shape::kBlock, Shape::kItems, Shape::kMinBlocks, Shape::kChains, StatusT, MATCH>;
   static std::once_flag once;
   static int ctas_per_sm = 1;
   std::call_once(once, [&] {
@@ -528,6 +589,25 @@ cudaError_t launch_onesweep_passes(typename Tr::Bits* keys, typename Tr::Bits* t
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
+}
+
+template <class Tr, typename StatusT>
+cudaError_t launch_onesweep_variant(typename Tr::Bits* keys, typename Tr::Bits* tmp, RadixState* st, char* tbase,
+                                    const RadixLayout& L, uint32_t n, bool use_tma, cudaStream_t stream,
+                                    LaunchRecorder* rec) {
+#define MGS_LAUNCH(S, M) launch_onesweep_passes<Tr, S, StatusT, M>(keys, tmp, st, tbase, L, n, use_tma, stream, rec)
+  if (rank_mode() == 1) return MGS_LAUNCH(kDefaultShape, 1);
+  if (rank_mode() == 0) return MGS_LAUNCH(kDefaultShape, 0);
+  switch (onesweep_shape()) {
+    case 0: return MGS_LAUNCH(0, 2);
+    case 1: return MGS_LAUNCH(1, 2);
+    case 3: return MGS_LAUNCH(3, 2);
+    case 4: return MGS_LAUNCH(4, 2);
+    case 5: return MGS_LAUNCH(5, 2);
+    case 6: return MGS_LAUNCH(6, 2);
+    default: return MGS_LAUNCH(2, 2);
+  }
+#undef MGS_LAUNCH
 }
 
 template <class Tr>
@@ -557,13 +637,10 @@ cudaError_t radix_sort_typed(typename Tr::Bits* keys, size_t n, void* temp, size
   if (e != cudaSuccess) return e;
 
   const bool use_tma = (reinterpret_cast<uintptr_t>(keys) & 15u) == 0;
-  const int mode = rank_mode();  // default: shared-memory peer masks
   if (L.status_bytes == 4) {
-    if (mode == 0) e = launch_onesweep_passes<Tr, uint32_t, 0>(keys, tmp, st, tb, L, n32, use_tma, stream, rec);
-    else if (mode == 1) e = launch_onesweep_passes<Tr, uint32_t, 1>(keys, tmp, st, tb, L, n32, use_tma, stream, rec);
-    else e = launch_onesweep_passes<Tr, uint32_t, 2>(keys, tmp, st, tb, L, n32, use_tma, stream, rec);
+    e = launch_onesweep_variant<Tr, uint32_t>(keys, tmp, st, tb, L, n32, use_tma, stream, rec);
   } else {
-    e = launch_onesweep_passes<Tr, unsigned long long, 2>(keys, tmp, st, tb, L, n32, use_tma, stream, rec);
+    e = launch_onesweep_variant<Tr, unsigned long long>(keys, tmp, st, tb, L, n32, use_tma, stream, rec);
   }
   if (e != cudaSuccess) return e;
 

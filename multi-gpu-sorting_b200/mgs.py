@@ -92,6 +92,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "mgs_merge_device": ([c_void, c_int, c_void, c_size, c_void, c_size, c_void, c_void, c_size, c_void], c_int),
         "mgs_kway_merge_device": ([c_void, c_int, ctypes.POINTER(c_void), ctypes.POINTER(c_size), c_int, c_void,
                                    c_void, c_size, c_void], c_int),
+        "mgs_gowanlock_sort": ([c_void, c_int, c_void, c_size, c_size, c_size, c_size, c_int], c_int),
+        "mgs_ctx_phase_seconds": ([c_void, ctypes.c_char_p, ctypes.POINTER(ctypes.c_double)], c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -156,7 +158,7 @@ def generate(dtype, distribution: str, seed: int, n: int, out: np.ndarray | None
 
 def sort_device_noalloc(d_keys: int, n: int, dtype, stream: int = 0) -> None:
     """mgs_sort_device_noalloc: the device sort without any allocation (fixed 32 MiB scratch in
-    the library's device image; at most 7,890,880 4-byte or 3,945,440 8-byte keys). For callers
+    the library's device image; at most 2^22 4-byte or 2^21 8-byte keys). For callers
     that cannot call cudaMalloc. Calls that overlap on one GPU race."""
     lib = load_library()
     _check(lib.mgs_sort_device_noalloc(dtype_code(dtype), ctypes.c_void_p(d_keys), int(n),
@@ -256,6 +258,20 @@ class Context:
         _check(self._lib.mgs_kway_merge_device(self.handle, dtype_code(dtype), rp, lp, k, ctypes.c_void_p(d_out),
                                                ctypes.c_void_p(d_temp or None), int(temp_bytes),
                                                ctypes.c_void_p(stream or None)))
+
+    # --- GowanlockSort with one GPU: out-of-core chunk pipeline ---
+    def gowanlock_sort(self, keys: np.ndarray, chunk_size: int = 0, merge_group_size: int = 0, num_buffers: int = 2,
+                       merge_on_gpu: bool = True) -> None:
+        """GowanlockSort<T>(&keys, chunk_size, merge_group_size, num_buffers, gpus) (src/gowanlock_sort.cuh:395)."""
+        assert keys.flags.c_contiguous
+        _check(self._lib.mgs_gowanlock_sort(self.handle, dtype_code(keys.dtype), keys.ctypes.data_as(ctypes.c_void_p),
+                                            keys.size, int(chunk_size), int(merge_group_size), int(num_buffers),
+                                            0 if merge_on_gpu else 1))
+
+    def phase_seconds(self, phase: str) -> float:
+        v = ctypes.c_double()
+        _check(self._lib.mgs_ctx_phase_seconds(self.handle, phase.encode(), ctypes.byref(v)))
+        return v.value
 
     def synchronize(self) -> None:
         _check(self._lib.mgs_ctx_synchronize(self.handle))

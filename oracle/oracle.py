@@ -62,6 +62,8 @@ def ref_lib() -> ctypes.CDLL:
         lib.ref_phase_seconds.argtypes = [ctypes.c_char_p]
         lib.ref_phase_seconds.restype = ctypes.c_double
         lib.ref_num_procs.restype = i
+        lib.ref_cub_sort_device_ms.argtypes = [i, v, s, v, s, ctypes.POINTER(s)]
+        lib.ref_cub_sort_device_ms.restype = ctypes.c_double
         _ref = lib
     return _ref
 
@@ -165,6 +167,15 @@ def ref_gowanlock_sort(a: np.ndarray, chunk_size: int = 0, merge_group_size: int
                        device: int = 0, threads: int = 8) -> None:
     assert ref_lib().ref_gowanlock_sort(code(a), _ptr(a), a.size, chunk_size, merge_group_size, num_buffers,
                                         device, threads) == 0
+
+
+def ref_cub_sort_device_ms(dtype_code: int, d_keys: int, n: int, d_temp: int = 0, temp_bytes: int = 0):
+    """cub::DeviceRadixSort::SortKeys on device keys (src/local_gpu_sort_algorithm_benchmark.cu:51-67).
+    Returns (ms, temp bytes CUB needs); ms < 0 when only the size was queried."""
+    need = ctypes.c_size_t()
+    ms = ref_lib().ref_cub_sort_device_ms(dtype_code, ctypes.c_void_p(d_keys), n, ctypes.c_void_p(d_temp or None),
+                                          temp_bytes, ctypes.byref(need))
+    return ms, need.value
 
 
 def ref_num_procs() -> int:

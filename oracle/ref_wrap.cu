@@ -9,8 +9,13 @@
 //   ref_gowanlock_sort    SetupGowanlockSort + GowanlockSort<T>    src/gowanlock_sort.cuh:117-125,395-483
 //   ref_gnu_parallel_sort the "gnu_parallel" algorithm branch      src/sort_benchmark.cu:314-319
 //   ref_multiway_merge    __gnu_parallel::multiway_merge call      src/local_cpu_multiway_merge_benchmark.cu:255-256
-//   ref_sort_phase_seconds TimeDurations "sort_phase"              src/time_durations.cuh
+//   ref_cub_sort_device_ms cub::DeviceRadixSort::SortKeys on device keys, the
+//                          library call the reference times in
+//                          src/local_gpu_sort_algorithm_benchmark.cu:51-67 (CUDA events)
+//   ref_phase_seconds     TimeDurations phase                       src/time_durations.cuh
 #include <omp.h>
+
+#include <cub/cub.cuh>
 
 #include <cstdint>
 #include <cstring>
@@ -106,6 +111,35 @@ int ref_multiway_merge(int dtype, const void* const* runs, const size_t* lens, i
                                    std::less<T>());
     TimeDurations::Get()->Toc("merge_phase");
   });
+}
+
+// Sorts d_keys[0..n) (device) with cub::DeviceRadixSort::SortKeys, in place as the reference's
+// benchmark does (same pointer for input and output), and returns the CUDA-event time in ms of
+// the sort alone. d_temp must hold the bytes CUB asks for; temp_bytes 0 = query them (returned
+// through *need).
+double ref_cub_sort_device_ms(int dtype, void* d_keys, size_t n, void* d_temp, size_t temp_bytes, size_t* need) {
+  double ms = -1.0;
+  dispatch(dtype, [&](auto tag) {
+    using T = decltype(tag);
+    T* p = static_cast<T*>(d_keys);
+    size_t bytes = 0;
+    cub::DeviceRadixSort::SortKeys(nullptr, bytes, p, p, n, 0, int(sizeof(T) * 8));
+    if (need) *need = bytes;
+    if (temp_bytes < bytes || d_temp == nullptr) return;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaEventRecord(a);
+    cub::DeviceRadixSort::SortKeys(d_temp, bytes, p, p, n, 0, int(sizeof(T) * 8));
+    cudaEventRecord(b);
+    cudaEventSynchronize(b);
+    float t = 0.f;
+    cudaEventElapsedTime(&t, a, b);
+    ms = t;
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+  });
+  return ms;
 }
 
 double ref_phase_seconds(const char* phase) { return TimeDurations::Get()->durations[phase].count(); }

@@ -18,7 +18,7 @@ pytestmark = pytest.mark.gpu
 
 torch = pytest.importorskip("torch")
 
-MAX_KEYS = {4: 7890880, 8: 3945440}
+MAX_KEYS = {4: 1 << 22, 8: 1 << 21}
 
 
 def noalloc_fn(mgs):
@@ -36,6 +36,7 @@ def on_device(a):
 
 @pytest.mark.parametrize("dtype,dist,n", [
     ("u32", "uniform", 1_000_003),
+    ("u64", "uniform", 1 << 21),
     ("f32", "full-uniform-specials", 777_777),
     ("u64", "full-uniform", 500_001),
     ("i32", "zipf", 65_537),
