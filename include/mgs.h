@@ -159,6 +159,22 @@ int mgs_merge_device(mgs_ctx* ctx, int dtype, const void* d_a, size_t na, const 
 int mgs_kway_merge_device(mgs_ctx* ctx, int dtype, const void* const* d_runs, const size_t* lens, int k, void* d_out,
                           void* d_temp, size_t temp_bytes, void* stream);
 
+/* ---- batched segmented sort (no counterpart in the reference; the batched form
+ * of the device sort) --------------------------------------------------------
+ * Every segment [d_offsets[s], d_offsets[s+1]) of d_keys (device, n keys) is
+ * sorted on its own, ascending and stably, in the same order as
+ * mgs_sort_device. d_offsets: num_segments + 1 device uint64 values, each
+ * segment inside [0, n). Segments of up to 256 keys are sorted by one warp,
+ * up to one tile (16384 4-byte / 8192 8-byte keys) by one CTA entirely in
+ * shared memory, both classes in one persistent launch; longer segments go
+ * through the onesweep passes all at once. The launch sequence does not read
+ * anything back to the host (stream-ordered, capturable in a CUDA graph).
+ * Invalid offsets (decreasing, or beyond n) leave that segment unsorted and
+ * make the next mgs_ctx_synchronize return MGS_ERR_INVALID. Asynchronous. */
+int mgs_segmented_sort_temp_bytes(int dtype, size_t n, size_t num_segments, size_t* bytes);
+int mgs_segmented_sort_device(mgs_ctx* ctx, int dtype, void* d_keys, size_t n, const uint64_t* d_offsets,
+                              size_t num_segments, void* d_temp, size_t temp_bytes, void* stream);
+
 /* ---- GowanlockSort on one GPU: out-of-core chunk pipeline -------------------
  * (HET sort, src/gowanlock_sort.cuh:127-483). h_keys (host, pinned for full link
  * speed) is sorted in place. Phase 1 streams chunks of chunk_size keys through

@@ -41,6 +41,11 @@ int invalid(const char* msg) {
 
 int status_to_code(uint32_t status) {
   if (status == 0) return MGS_OK;
+  if (status == mgs::kStatusBadInput) {
+    set_last_error("device status 0x%x: invalid input found by a kernel (segment offsets out of order or range)",
+                   status);
+    return MGS_ERR_INVALID;
+  }
   set_last_error("device status 0x%x: a bounded device-side wait gave up (%s%s%s)", status,
                  (status & mgs::kStatusLookbackTimeout) ? "look-back " : "",
                  (status & mgs::kStatusTmaTimeout) ? "tma " : "", (status & mgs::kStatusQueueTimeout) ? "queue " : "");
@@ -399,6 +404,45 @@ int mgs_merge_device(mgs_ctx* ctx, int dtype, const void* d_a, size_t na, const 
   const void* runs[2] = {d_a, d_b};
   const size_t lens[2] = {na, nb};
   return mgs_kway_merge_device(ctx, dtype, runs, lens, 2, d_out, d_temp, temp_bytes, stream);
+}
+
+int mgs_segmented_sort_temp_bytes(int dtype, size_t n, size_t num_segments, size_t* bytes) {
+  if (!bytes) return invalid("mgs_segmented_sort_temp_bytes: bytes is null");
+  if (mgs::dtype_bytes(dtype) == 0) return invalid("mgs_segmented_sort_temp_bytes: unknown dtype");
+  if (n > kMaxDeviceSortKeys || num_segments >= kMaxDeviceSortKeys)
+    return invalid("mgs_segmented_sort_temp_bytes: n and num_segments must be below 2^32");
+  *bytes = mgs::segmented_sort_temp_bytes(dtype, n, num_segments);
+  return MGS_OK;
+}
+
+int mgs_segmented_sort_device(mgs_ctx* ctx, int dtype, void* d_keys, size_t n, const uint64_t* d_offsets,
+                              size_t num_segments, void* d_temp, size_t temp_bytes, void* stream) {
+  if (!ctx) return invalid("mgs_segmented_sort_device: ctx is null");
+  const size_t w = mgs::dtype_bytes(dtype);
+  if (w == 0) return invalid("mgs_segmented_sort_device: unknown dtype");
+  if (n == 0 || num_segments == 0) return MGS_OK;
+  if (!d_keys || !d_offsets) return invalid("mgs_segmented_sort_device: null pointer");
+  if (reinterpret_cast<uintptr_t>(d_keys) % w != 0) return invalid("mgs_segmented_sort_device: d_keys is not key-aligned");
+  if (n > kMaxDeviceSortKeys || num_segments >= kMaxDeviceSortKeys)
+    return invalid("mgs_segmented_sort_device: n and num_segments must be below 2^32");
+  Context& c = ctx->impl;
+  DeviceGuard g(c.device);
+  const size_t need = mgs::segmented_sort_temp_bytes(dtype, n, num_segments);
+  if (d_temp == nullptr) {
+    cudaError_t e = c.reserve(need);
+    if (e != cudaSuccess) return cuda_fail(e, "mgs_segmented_sort_device: arena");
+    d_temp = c.arena;
+    temp_bytes = c.arena_bytes;
+  } else if (temp_bytes < need) {
+    set_last_error("mgs_segmented_sort_device: d_temp holds %zu bytes, %zu needed", temp_bytes, need);
+    return MGS_ERR_INVALID;
+  }
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c.compute;
+  cudaError_t e = mgs::segmented_sort(dtype, d_keys, n, d_offsets, num_segments, d_temp, temp_bytes, s, c.d_status,
+                                      &c.recorder);
+  if (e != cudaSuccess) return cuda_fail(e, "mgs_segmented_sort_device");
+  mgs::clear_last_error();
+  return MGS_OK;
 }
 
 int mgs_gowanlock_sort(mgs_ctx* ctx, int dtype, void* h_keys, size_t n, size_t chunk_size, size_t merge_group_size,

@@ -201,6 +201,7 @@ struct OnesweepSmem {
   uint32_t scan_tmp[kWarps + 1];
   uint32_t tile_id[2];
   alignas(8) uint64_t bar[2];
+  alignas(16) unsigned char span[2][48];  // TileSpan of the current / prefetched tile
 };
 
 // Peer mask of lanes holding the same digit (the warp multisplit step).
@@ -234,20 +235,24 @@ __device__ __forceinline__ uint32_t digit_peers(uint32_t d, bool ok, uint32_t* m
   }
 }
 
-// One tile: count, publish, rank into shared memory in digit order, look back,
-// scatter. Warp w owns tile positions [w*32*ITEMS, (w+1)*32*ITEMS); item i of
-// lane l is position w*32*ITEMS + i*32 + l, so (warp, item, lane) is input
-// order. With CHAINS = 2 the warp's items split into two halves that are
-// ranked as independent chains (own counters and masks), interleaved so that
-// their shared-memory latencies overlap; the second half's counters start
-// after the first half's keys of the same digit.
-template <class Tr, int BLOCK, int ITEMS, int CHAINS, typename StatusT, int MATCH, bool FULL>
-__device__ __forceinline__ void onesweep_tile(OnesweepSmem<Tr, BLOCK, ITEMS, CHAINS>& sm, typename Tr::Bits* skeys,
-                                              RadixState* __restrict__ st, StatusT* __restrict__ lb_cur,
-                                              typename Tr::Bits* __restrict__ dst, uint32_t tile, uint32_t valid,
-                                              uint32_t n, int pass) {
+// Phases 1-2 of ranking a tile held in shared memory: stable rank of `valid`
+// keys of `src` by the digit of `pass`, written in digit order into `dst`
+// (dst may be src). Warp w owns tile positions [w*32*ITEMS, (w+1)*32*ITEMS);
+// item i of lane l is position w*32*ITEMS + i*32 + l, so (warp, item, lane) is
+// input order. With CHAINS = 2 the warp's items split into two halves ranked as
+// independent chains (own counters and masks), interleaved so that their
+// shared-memory latencies overlap; the second half's counters start after the
+// first half's keys of the same digit. on_counts(count) runs on threads
+// d < 256 with the tile's count of digit d before the ranks are formed (the
+// onesweep publishes its look-back aggregate there). With ALLOW_SKIP, a digit
+// shared by every key makes the pass the identity: nothing is written and the
+// function returns true (block-uniform). sm.tile_start receives the exclusive
+// scan of the digit counts. The caller synchronizes before reading dst.
+template <class Tr, int BLOCK, int ITEMS, int CHAINS, int MATCH, bool FULL, bool ALLOW_SKIP, class OnCounts>
+__device__ __forceinline__ bool rank_tile(OnesweepSmem<Tr, BLOCK, ITEMS, CHAINS>& sm, const typename Tr::Bits* src,
+                                          typename Tr::Bits* dst, uint32_t valid, int pass, uint32_t* tile_count_out,
+                                          OnCounts on_counts) {
   using Bits = typename Tr::Bits;
-  using LW = LookbackWord<StatusT>;
   constexpr int kTile = BLOCK * ITEMS;
   constexpr int kChains = (BLOCK / 32) * CHAINS;
   constexpr int kPerChain = ITEMS / CHAINS;
@@ -256,25 +261,28 @@ __device__ __forceinline__ void onesweep_tile(OnesweepSmem<Tr, BLOCK, ITEMS, CHA
   const int warp = tid >> 5, lane = tid & 31;
   const int wbase = warp * 32 * ITEMS;
 
+  for (int i = tid; i < kChains * kRadix; i += BLOCK) sm.ccount[i] = 0u;
+  __syncthreads();
   // Phase 1: per-chain digit counts.
   Bits key[ITEMS];
 #pragma unroll
   for (int i = 0; i < ITEMS; ++i) {
     const uint32_t idx = wbase + i * 32 + lane;
-    key[i] = skeys[idx];
+    key[i] = src[idx];
     uint32_t* cc = sm.ccount + (warp * CHAINS + i / kPerChain) * kRadix;
     if (FULL || idx < valid) atomicAdd(&cc[Tr::Digit(key[i], pass)], 1u);
   }
   __syncthreads();
 
-  // Per digit: publish the tile's count for the look-back right away, then seed
-  // every chain's counter with the tile position of its first key of that digit.
   uint32_t tile_count = 0;
   if (tid < kRadix) {
 #pragma unroll
     for (int c = 0; c < kChains; ++c) tile_count += sm.ccount[c * kRadix + tid];
-    StatusT* slot = lb_cur + size_t(tile) * kRadix + tid;
-    LW::store(slot, tile == 0 ? (LW::kPrefix | StatusT(tile_count)) : StatusT(tile_count + 1u));
+    on_counts(tile_count);
+  }
+  *tile_count_out = tile_count;
+  if (ALLOW_SKIP) {
+    if (__syncthreads_or(tid < kRadix && tile_count == valid)) return true;
   }
   uint32_t total;
   const uint32_t tstart = block_exclusive_scan<BLOCK>(tid < kRadix ? tile_count : 0u, sm.scan_tmp, &total);
@@ -333,23 +341,55 @@ __device__ __forceinline__ void onesweep_tile(OnesweepSmem<Tr, BLOCK, ITEMS, CHA
     __syncwarp();
 #pragma unroll
     for (int h = 0; h < CHAINS; ++h)
-      if (ok[h] && pos[h] < uint32_t(kTile)) skeys[pos[h]] = key[h * kPerChain + j];
+      if (ok[h] && pos[h] < uint32_t(kTile)) dst[pos[h]] = key[h * kPerChain + j];
   }
+  return false;
+}
 
-  // Decoupled look-back: one thread per digit walks back over earlier tiles,
-  // summing their aggregates until it meets an inclusive prefix. Statuses of
-  // kLookahead predecessors are fetched per round (independent loads).
+// Where one onesweep tile's keys come from and go to. For the plain sort the
+// whole array is one segment; for the segmented sort every large segment is
+// its own run of tiles (a tile never spans two segments).
+template <class Tr>
+struct alignas(16) TileSpan {
+  const typename Tr::Bits* src;  // the segment's first key in the source buffer
+  typename Tr::Bits* dst;        // the segment's first key in the destination buffer
+  uint32_t first_tile;           // global id of the segment's first tile (look-back stops there)
+  uint32_t seg_len;              // keys in the segment
+  const uint32_t* bucket;        // 256 bucket starts of this pass within the segment
+};
+
+// One tile: rank in shared memory (publishing the tile's digit counts for the
+// look-back as soon as they are known), look back over the segment's earlier
+// tiles, scatter the digit runs.
+template <class Tr, int BLOCK, int ITEMS, int CHAINS, typename StatusT, int MATCH, bool FULL>
+__device__ __forceinline__ void onesweep_tile(OnesweepSmem<Tr, BLOCK, ITEMS, CHAINS>& sm, typename Tr::Bits* skeys,
+                                              RadixState* __restrict__ st, StatusT* __restrict__ lb_cur,
+                                              const TileSpan<Tr>& span, uint32_t tile, uint32_t valid, int pass) {
+  using Bits = typename Tr::Bits;
+  using LW = LookbackWord<StatusT>;
+  const int tid = threadIdx.x;
+  uint32_t tile_count = 0;
+  rank_tile<Tr, BLOCK, ITEMS, CHAINS, MATCH, FULL, false>(
+      sm, skeys, skeys, valid, pass, &tile_count, [&](uint32_t count) {
+        StatusT* slot = lb_cur + size_t(tile) * kRadix + tid;
+        LW::store(slot, tile == span.first_tile ? (LW::kPrefix | StatusT(count)) : StatusT(count + 1u));
+      });
+
+  // Decoupled look-back: one thread per digit walks back over earlier tiles of
+  // the segment, summing their aggregates until it meets an inclusive prefix.
+  // Statuses of kLookahead predecessors are fetched per round.
   if (tid < kRadix) {
     StatusT excl = 0;
-    if (tile > 0) {
+    if (tile > span.first_tile) {
+      const long long first = span.first_tile;
       long long jt = static_cast<long long>(tile) - 1;
       uint32_t spins = 0;
       bool done = false;
-      while (!done && jt >= 0) {
+      while (!done && jt >= first) {
         StatusT sv[kLookahead];
 #pragma unroll
         for (int q = 0; q < kLookahead; ++q)
-          sv[q] = (jt - q >= 0) ? LW::load(lb_cur + size_t(jt - q) * kRadix + tid) : (LW::kPrefix | StatusT(0));
+          sv[q] = (jt - q >= first) ? LW::load(lb_cur + size_t(jt - q) * kRadix + tid) : (LW::kPrefix | StatusT(0));
         int used = 0;
 #pragma unroll
         for (int q = 0; q < kLookahead; ++q) {
@@ -375,7 +415,7 @@ __device__ __forceinline__ void onesweep_tile(OnesweepSmem<Tr, BLOCK, ITEMS, CHA
       }
       LW::store(lb_cur + size_t(tile) * kRadix + tid, LW::kPrefix | (excl + tile_count));
     }
-    sm.gbase[tid] = st->bucket_start[pass][tid] + uint32_t(excl) - sm.tile_start[tid];
+    sm.gbase[tid] = span.bucket[tid] + uint32_t(excl) - sm.tile_start[tid];
   }
   __syncthreads();
 
@@ -387,17 +427,47 @@ __device__ __forceinline__ void onesweep_tile(OnesweepSmem<Tr, BLOCK, ITEMS, CHA
     if (FULL || idx < valid) {
       const Bits k = skeys[idx];
       const uint32_t gpos = sm.gbase[Tr::Digit(k, pass)] + idx;
-      if (gpos < n) dst[gpos] = k;
+      if (gpos < span.seg_len) span.dst[gpos] = k;
     }
   }
 }
 
-template <class Tr, int BLOCK, int ITEMS, int MINB, int CHAINS, typename StatusT, int MATCH>
+// Large segments of a segmented sort, as seen by the onesweep kernels.
+struct SegLarge {
+  const unsigned long long* offsets;  // segment offsets (nseg + 1)
+  const uint32_t* ids;                // large segment ids, in segment order
+  const uint32_t* tile_prefix;        // first global tile of each large segment (n_large + 1)
+  const uint32_t* counts;             // [n_small, n_medium, n_large, large_tiles]
+  const uint32_t* bucket;             // [n_large][P][256] bucket starts
+};
+
+template <class Tr>
+__device__ __forceinline__ TileSpan<Tr> seg_span(const SegLarge& sg, const typename Tr::Bits* src,
+                                                 typename Tr::Bits* dst, uint32_t tile, int pass) {
+  const uint32_t nl = sg.counts[2];
+  uint32_t lo = 0, hi = nl;  // largest s with tile_prefix[s] <= tile
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (sg.tile_prefix[mid] <= tile) lo = mid; else hi = mid;
+  }
+  const uint32_t seg = sg.ids[lo];
+  const unsigned long long b = sg.offsets[seg];
+  TileSpan<Tr> sp;
+  sp.src = src + b;
+  sp.dst = dst + b;
+  sp.first_tile = sg.tile_prefix[lo];
+  sp.seg_len = uint32_t(sg.offsets[seg + 1] - b);
+  sp.bucket = sg.bucket + (size_t(lo) * Tr::kPasses + pass) * kRadix;
+  return sp;
+}
+
+template <class Tr, int BLOCK, int ITEMS, int MINB, int CHAINS, typename StatusT, int MATCH, bool SEG>
 __global__ __launch_bounds__(BLOCK, MINB) void radix_onesweep_kernel(typename Tr::Bits* buf0, typename Tr::Bits* buf1,
                                                                      RadixState* __restrict__ st,
                                                                      StatusT* __restrict__ lb_cur,
                                                                      StatusT* __restrict__ lb_next, uint32_t n,
-                                                                     uint32_t num_tiles, int pass, int use_tma) {
+                                                                     uint32_t num_tiles_arg, int pass, int use_tma,
+                                                                     SegLarge sg) {
   using Bits = typename Tr::Bits;
   using Smem = OnesweepSmem<Tr, BLOCK, ITEMS, CHAINS>;
   constexpr int kTile = Smem::kTile;
@@ -407,6 +477,7 @@ __global__ __launch_bounds__(BLOCK, MINB) void radix_onesweep_kernel(typename Tr
   extern __shared__ __align__(128) unsigned char smem_raw[];
   Smem& sm = *reinterpret_cast<Smem*>(smem_raw);
   const int tid = threadIdx.x;
+  const uint32_t num_tiles = SEG ? sg.counts[3] : num_tiles_arg;
 
   // The next pass uses the other look-back array; clear it (grid-stride).
   if (lb_next != nullptr) {
@@ -419,11 +490,23 @@ __global__ __launch_bounds__(BLOCK, MINB) void radix_onesweep_kernel(typename Tr
   const Bits* src = sel ? buf1 : buf0;
   Bits* dst = sel ? buf0 : buf1;
 
+  auto span_of = [&](uint32_t t) {
+    if (SEG) return seg_span<Tr>(sg, src, dst, t, pass);
+    TileSpan<Tr> sp{src, dst, 0u, n, st->bucket_start[pass]};
+    return sp;
+  };
+  auto tma_ok = [&](const TileSpan<Tr>& sp, uint32_t t) {
+    const size_t off = size_t(t - sp.first_tile) * kTile;
+    return use_tma && off + kTile <= sp.seg_len && ((reinterpret_cast<uintptr_t>(sp.src + off) & 15u) == 0);
+  };
+
   // Persistent CTA: tiles come in launch order from an atomic counter; the
   // next tile is claimed and its TMA bulk copy issued before the current tile
   // is ranked, so loads overlap compute. A CTA's current tile is always older
   // than its prefetched one, so the oldest unfinished tile is always being
   // processed and the look-back makes progress.
+  static_assert(sizeof(TileSpan<Tr>) <= sizeof(sm.span[0]), "span slot");
+  TileSpan<Tr>* spans = reinterpret_cast<TileSpan<Tr>*>(sm.span);
   if (MATCH == 2)
     for (int i = tid; i < kChains * 2 * kRadix; i += BLOCK) sm.masks[i] = 0u;
   if (tid == 0) {
@@ -432,9 +515,13 @@ __global__ __launch_bounds__(BLOCK, MINB) void radix_onesweep_kernel(typename Tr
     fence_mbar_init();
     const uint32_t t = atomicAdd(&st->tile_counter[pass], 1u);
     sm.tile_id[0] = t;
-    if (use_tma && t < num_tiles && size_t(t + 1) * kTile <= n) {
-      mbar_arrive_expect_tx(&sm.bar[0], kTileBytes);
-      bulk_copy_g2s(sm.keys[0], src + size_t(t) * kTile, kTileBytes, &sm.bar[0]);
+    if (t < num_tiles) {
+      const TileSpan<Tr> sp = span_of(t);
+      spans[0] = sp;
+      if (tma_ok(sp, t)) {
+        mbar_arrive_expect_tx(&sm.bar[0], kTileBytes);
+        bulk_copy_g2s(sm.keys[0], sp.src + size_t(t - sp.first_tile) * kTile, kTileBytes, &sm.bar[0]);
+      }
     }
   }
   __syncthreads();
@@ -446,17 +533,21 @@ __global__ __launch_bounds__(BLOCK, MINB) void radix_onesweep_kernel(typename Tr
     if (tid == 0) {
       const uint32_t t = atomicAdd(&st->tile_counter[pass], 1u);
       sm.tile_id[cur ^ 1] = t;
-      if (use_tma && t < num_tiles && size_t(t + 1) * kTile <= n) {
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        mbar_arrive_expect_tx(&sm.bar[cur ^ 1], kTileBytes);
-        bulk_copy_g2s(sm.keys[cur ^ 1], src + size_t(t) * kTile, kTileBytes, &sm.bar[cur ^ 1]);
+      if (t < num_tiles) {
+        const TileSpan<Tr> sp = span_of(t);
+        spans[cur ^ 1] = sp;
+        if (tma_ok(sp, t)) {
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+          mbar_arrive_expect_tx(&sm.bar[cur ^ 1], kTileBytes);
+          bulk_copy_g2s(sm.keys[cur ^ 1], sp.src + size_t(t - sp.first_tile) * kTile, kTileBytes, &sm.bar[cur ^ 1]);
+        }
       }
     }
-    for (int i = tid; i < kChains * kRadix; i += BLOCK) sm.ccount[i] = 0u;
+    const TileSpan<Tr> span = spans[cur];
     Bits* skeys = sm.keys[cur];
-    const size_t base = size_t(tile) * kTile;
-    const uint32_t valid = uint32_t(min(size_t(kTile), size_t(n) - base));
-    if (use_tma && valid == uint32_t(kTile)) {
+    const size_t base = size_t(tile - span.first_tile) * kTile;
+    const uint32_t valid = uint32_t(min(size_t(kTile), size_t(span.seg_len) - base));
+    if (tma_ok(span, tile)) {
       const bool arrived = mbar_wait_bounded(&sm.bar[cur], (parity >> cur) & 1u, kTmaWaitLimit);
       parity ^= 1u << cur;
       if (__syncthreads_or(!arrived)) {  // block-uniform exit when the copy never completed
@@ -464,16 +555,274 @@ __global__ __launch_bounds__(BLOCK, MINB) void radix_onesweep_kernel(typename Tr
         return;
       }
     } else {
-      for (uint32_t i = tid; i < valid; i += BLOCK) skeys[i] = src[base + i];
-      __syncthreads();
+      for (uint32_t i = tid; i < valid; i += BLOCK) skeys[i] = span.src[base + i];
     }
     if (valid == uint32_t(kTile)) {
-      onesweep_tile<Tr, BLOCK, ITEMS, CHAINS, StatusT, MATCH, true>(sm, skeys, st, lb_cur, dst, tile, valid, n, pass);
+      onesweep_tile<Tr, BLOCK, ITEMS, CHAINS, StatusT, MATCH, true>(sm, skeys, st, lb_cur, span, tile, valid, pass);
     } else {
-      onesweep_tile<Tr, BLOCK, ITEMS, CHAINS, StatusT, MATCH, false>(sm, skeys, st, lb_cur, dst, tile, valid, n, pass);
+      onesweep_tile<Tr, BLOCK, ITEMS, CHAINS, StatusT, MATCH, false>(sm, skeys, st, lb_cur, span, tile, valid, pass);
     }
     __syncthreads();
     cur ^= 1;
+  }
+}
+
+// ---------------------------------------------------------------- segmented -
+// Batched segmented sort: every segment [offsets[s], offsets[s+1]) of one key
+// array is sorted on its own (stably), all segments in a fixed number of
+// launches. Segments fall into size classes:
+//   small  (2..kSmallCap keys)  one warp each, LSD passes in warp-private
+//                               shared memory;
+//   medium (..one tile of keys) one CTA each, LSD passes entirely in shared
+//                               memory (load once, store once);
+//   large  (more than a tile)   the onesweep pipeline over all large segments
+//                               at once: per-segment histograms and bucket
+//                               starts, tiles that never span segments, and a
+//                               look-back that stops at the segment's first tile.
+// Small and medium segments share one persistent launch.
+constexpr uint32_t kSmallCap = 256;  // 32 lanes x 8 keys
+
+struct SegPlanHeader {
+  uint32_t counts[4];  // n_small, n_medium, n_large, large tiles
+  uint32_t work_counter;
+  uint32_t pad[3];
+};
+
+template <int BLOCK>
+__global__ __launch_bounds__(BLOCK) void seg_classify_kernel(const unsigned long long* __restrict__ offsets,
+                                                             uint32_t nseg, unsigned long long n, uint32_t tile,
+                                                             uint32_t medium_cap, SegPlanHeader* __restrict__ hdr,
+                                                             uint32_t* __restrict__ small_ids,
+                                                             uint32_t* __restrict__ medium_ids,
+                                                             uint32_t* __restrict__ large_ids,
+                                                             uint32_t* __restrict__ tile_prefix,
+                                                             uint32_t* __restrict__ d_status) {
+  __shared__ uint32_t tmp[BLOCK / 32 + 1];
+  uint32_t cnt_small = 0, cnt_medium = 0, cnt_large = 0, tiles = 0;
+  for (uint32_t base = 0; base < nseg; base += BLOCK) {
+    const uint32_t s = base + threadIdx.x;
+    unsigned long long len = 0;
+    if (s < nseg) {
+      const unsigned long long b = offsets[s], e = offsets[s + 1];
+      if (e < b || e > n) {
+        if (d_status) atomicOr(d_status, kStatusBadInput);
+      } else {
+        len = e - b;
+      }
+    }
+    const int cls = len <= 1 ? 0 : len <= kSmallCap ? 1 : len <= medium_cap ? 2 : 3;
+    uint32_t tot;
+    uint32_t ex = block_exclusive_scan<BLOCK>(cls == 1 ? 1u : 0u, tmp, &tot);
+    if (cls == 1) small_ids[cnt_small + ex] = s;
+    cnt_small += tot;
+    ex = block_exclusive_scan<BLOCK>(cls == 2 ? 1u : 0u, tmp, &tot);
+    if (cls == 2) medium_ids[cnt_medium + ex] = s;
+    cnt_medium += tot;
+    const uint32_t my_tiles = cls == 3 ? uint32_t((len + tile - 1) / tile) : 0u;
+    uint32_t ttot;
+    const uint32_t tex = block_exclusive_scan<BLOCK>(my_tiles, tmp, &ttot);
+    ex = block_exclusive_scan<BLOCK>(cls == 3 ? 1u : 0u, tmp, &tot);
+    if (cls == 3) {
+      large_ids[cnt_large + ex] = s;
+      tile_prefix[cnt_large + ex] = tiles + tex;
+    }
+    cnt_large += tot;
+    tiles += ttot;
+  }
+  if (threadIdx.x == 0) {
+    tile_prefix[cnt_large] = tiles;
+    hdr->counts[0] = cnt_small;
+    hdr->counts[1] = cnt_medium;
+    hdr->counts[2] = cnt_large;
+    hdr->counts[3] = tiles;
+    hdr->work_counter = 0;
+  }
+}
+
+// Sorts one small segment (len <= kSmallCap) with one warp: LSD passes of
+// 8-bit digits between two warp-private shared buffers; passes whose digit is
+// the same for every key are skipped.
+template <class Tr>
+__device__ __forceinline__ void warp_sort_small(typename Tr::Bits* __restrict__ keys, uint32_t len,
+                                                typename Tr::Bits* A, typename Tr::Bits* B, uint32_t* cnt,
+                                                uint32_t* mm) {
+  using Bits = typename Tr::Bits;
+  constexpr int kItems = kSmallCap / 32;
+  const int lane = threadIdx.x & 31;
+  const uint32_t lmask = lanemask_lt(), lmask_gt = lanemask_gt();
+  for (uint32_t i = lane; i < len; i += 32) A[i] = keys[i];
+  __syncwarp();
+  for (int pass = 0; pass < Tr::kPasses; ++pass) {
+#pragma unroll
+    for (int q = 0; q < 8; ++q) cnt[lane * 8 + q] = 0u;
+    __syncwarp();
+    Bits k[kItems];
+#pragma unroll
+    for (int j = 0; j < kItems; ++j) {
+      const uint32_t idx = j * 32 + lane;
+      k[j] = A[idx];
+      if (idx < len) atomicAdd(&cnt[Tr::Digit(k[j], pass)], 1u);
+    }
+    __syncwarp();
+    uint32_t c[8], local = 0;
+    bool uniform = false;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      c[q] = cnt[lane * 8 + q];
+      uniform |= (c[q] == len);
+      local += c[q];
+    }
+    uint32_t incl = local;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    uint32_t run = incl - local;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      cnt[lane * 8 + q] = run;
+      run += c[q];
+    }
+    if (__any_sync(0xffffffffu, uniform)) {
+      __syncwarp();
+      continue;  // identity permutation
+    }
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < kItems; ++j) {
+      const uint32_t idx = j * 32 + lane;
+      const bool ok = idx < len;
+      const uint32_t d = ok ? Tr::Digit(k[j], pass) : 0u;
+      uint32_t* m = mm + (j & 1) * kRadix;
+      if (ok) atomicOr(&m[d], 1u << lane);
+      __syncwarp();
+      const uint32_t peers = ok ? m[d] : 0u;
+      const uint32_t pos = ok ? cnt[d] + __popc(peers & lmask) : 0u;
+      __syncwarp();
+      if (ok && (peers & lmask_gt) == 0) {
+        cnt[d] = pos + 1u;
+        m[d] = 0u;
+      }
+      __syncwarp();
+      if (ok && pos < kSmallCap) B[pos] = k[j];
+    }
+    __syncwarp();
+    Bits* t = A;
+    A = B;
+    B = t;
+  }
+  for (uint32_t i = lane; i < len; i += 32) keys[i] = A[i];
+  __syncwarp();
+}
+
+template <class Tr, int BLOCK, int ITEMS, int MINB, int CHAINS, int MATCH>
+__global__ __launch_bounds__(BLOCK, MINB) void seg_small_medium_kernel(typename Tr::Bits* __restrict__ keys,
+                                                                       const unsigned long long* __restrict__ offsets,
+                                                                       SegPlanHeader* __restrict__ hdr,
+                                                                       const uint32_t* __restrict__ small_ids,
+                                                                       const uint32_t* __restrict__ medium_ids) {
+  using Bits = typename Tr::Bits;
+  using Smem = OnesweepSmem<Tr, BLOCK, ITEMS, CHAINS>;
+  constexpr int kWarps = BLOCK / 32;
+  constexpr int kChains = Smem::kChains;
+  static_assert(kWarps * kSmallCap <= Smem::kTile, "warp buffers fit in one tile buffer");
+  static_assert(CHAINS == 1, "one mask/counter region per warp");
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  Smem& sm = *reinterpret_cast<Smem*>(smem_raw);
+  __shared__ uint32_t s_work;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  for (int i = tid; i < kChains * 2 * kRadix; i += BLOCK) sm.masks[i] = 0u;
+  const uint32_t n_small = hdr->counts[0], n_medium = hdr->counts[1];
+  const uint32_t n_items = n_medium + (n_small + kWarps - 1) / kWarps;
+  for (;;) {
+    __syncthreads();
+    if (tid == 0) s_work = atomicAdd(&hdr->work_counter, 1u);
+    __syncthreads();
+    const uint32_t work = s_work;
+    if (work >= n_items) break;
+    if (work < n_medium) {
+      const uint32_t seg = medium_ids[work];
+      const unsigned long long b = offsets[seg];
+      const uint32_t len = uint32_t(offsets[seg + 1] - b);
+      Bits* g = keys + b;
+      for (uint32_t i = tid; i < len; i += BLOCK) sm.keys[0][i] = g[i];
+      int cur = 0;
+      for (int pass = 0; pass < Tr::kPasses; ++pass) {
+        uint32_t tc;
+        const bool skipped = rank_tile<Tr, BLOCK, ITEMS, CHAINS, MATCH, false, true>(
+            sm, sm.keys[cur], sm.keys[cur ^ 1], len, pass, &tc, [](uint32_t) {});
+        __syncthreads();
+        if (!skipped) cur ^= 1;
+      }
+      for (uint32_t i = tid; i < len; i += BLOCK) g[i] = sm.keys[cur][i];
+    } else {
+      const uint32_t idx = (work - n_medium) * kWarps + warp;
+      if (idx < n_small) {
+        const uint32_t seg = small_ids[idx];
+        const unsigned long long b = offsets[seg];
+        warp_sort_small<Tr>(keys + b, uint32_t(offsets[seg + 1] - b), sm.keys[0] + warp * kSmallCap,
+                            sm.keys[1] + warp * kSmallCap, sm.ccount + warp * kRadix, sm.masks + warp * 2 * kRadix);
+      }
+    }
+  }
+}
+
+// Per large segment and pass: digit counts (one read of the large segments),
+// and the first look-back array cleared.
+template <class Tr, int BLOCK>
+__global__ __launch_bounds__(BLOCK) void seg_histogram_kernel(const typename Tr::Bits* __restrict__ keys,
+                                                              SegLarge sg, uint32_t tile,
+                                                              uint32_t* __restrict__ seg_hist,
+                                                              uint32_t* __restrict__ lb0) {
+  using Bits = typename Tr::Bits;
+  constexpr int P = Tr::kPasses;
+  __shared__ uint32_t h[P * kRadix];
+  __shared__ uint32_t s_seg, s_first;
+  const uint32_t num_tiles = sg.counts[3];
+  for (size_t i = size_t(blockIdx.x) * BLOCK + threadIdx.x; i < size_t(num_tiles) * kRadix;
+       i += size_t(gridDim.x) * BLOCK)
+    lb0[i] = 0u;
+  for (uint32_t t = blockIdx.x; t < num_tiles; t += gridDim.x) {
+    for (int i = threadIdx.x; i < P * kRadix; i += BLOCK) h[i] = 0u;
+    if (threadIdx.x == 0) {
+      uint32_t lo = 0, hi = sg.counts[2];
+      while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (sg.tile_prefix[mid] <= t) lo = mid; else hi = mid;
+      }
+      s_seg = lo;
+      s_first = sg.tile_prefix[lo];
+    }
+    __syncthreads();
+    const uint32_t si = s_seg;
+    const unsigned long long b = sg.offsets[sg.ids[si]];
+    const uint32_t len = uint32_t(sg.offsets[sg.ids[si] + 1] - b);
+    const uint32_t off = (t - s_first) * tile;
+    const uint32_t cnt = min(tile, len - off);
+    const Bits* src = keys + b + off;
+    for (uint32_t i = threadIdx.x; i < cnt; i += BLOCK) {
+      const Bits o = Tr::Ordered(src[i]);
+#pragma unroll
+      for (int p = 0; p < P; ++p) atomicAdd(&h[p * kRadix + (uint32_t(o >> (8 * p)) & 0xFFu)], 1u);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < P * kRadix; i += BLOCK)
+      if (h[i]) atomicAdd(&seg_hist[size_t(si) * P * kRadix + i], h[i]);
+    __syncthreads();
+  }
+}
+
+template <int P>
+__global__ __launch_bounds__(kRadix) void seg_scan_kernel(const uint32_t* __restrict__ counts,
+                                                          const uint32_t* __restrict__ seg_hist,
+                                                          uint32_t* __restrict__ seg_bucket) {
+  __shared__ uint32_t tmp[kRadix / 32 + 1];
+  const uint32_t units = counts[2] * P;
+  for (uint32_t u = blockIdx.x; u < units; u += gridDim.x) {
+    uint32_t total;
+    const uint32_t c = seg_hist[size_t(u) * kRadix + threadIdx.x];
+    seg_bucket[size_t(u) * kRadix + threadIdx.x] = block_exclusive_scan<kRadix>(c, tmp, &total);
   }
 }
 
@@ -567,8 +916,8 @@ cudaError_t launch_onesweep_passes(typename Tr::Bits* keys, typename Tr::Bits* t
                                    LaunchRecorder* rec) {
   using Shape = OnesweepShape<sizeof(typename Tr::Bits), SHAPE>;
   using Smem = OnesweepSmem<Tr, Shape::kBlock, Shape::kItems, Shape::kChains>;
-  auto kernel =
-      radix_onesweep_kernel<Tr, Shape::kBlock, Shape::kItems, Shape::kMinBlocks, Shape::kChains, StatusT, MATCH>;
+  auto kernel = radix_onesweep_kernel<Tr, Shape::kBlock, Shape::kItems, Shape::kMinBlocks, Shape::kChains, StatusT,
+                                      MATCH, false>;
   static std::once_flag once;
   static int ctas_per_sm = 1;
   std::call_once(once, [&] {
@@ -585,7 +934,7 @@ cudaError_t launch_onesweep_passes(typename Tr::Bits* keys, typename Tr::Bits* t
     StatusT* next = (p + 1 < Tr::kPasses) ? lb[(p + 1) & 1] : nullptr;
     cudaError_t e = launch_kernel(rec, "radix_onesweep", kernel, dim3(unsigned(grid)), dim3(Shape::kBlock),
                                   sizeof(Smem), stream, keys, tmp, st, cur, next, n, uint32_t(L.num_tiles), p,
-                                  use_tma ? 1 : 0);
+                                  use_tma ? 1 : 0, SegLarge{});
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
@@ -649,6 +998,113 @@ cudaError_t radix_sort_typed(typename Tr::Bits* keys, size_t n, void* temp, size
                        tmp, st, n32, d_status);
 }
 
+// ---------------------------------------------------------------- segmented host
+struct SegLayout {
+  size_t state_off, hdr_off, small_off, medium_off, large_off, prefix_off, hist_off, bucket_off, lb0_off, lb1_off,
+      keys_off, total;
+  size_t max_large, max_tiles, hist_bytes;
+};
+
+template <class Tr>
+SegLayout seg_layout(size_t n, size_t nseg) {
+  constexpr int w = int(sizeof(typename Tr::Bits));
+  constexpr size_t tile = shape_tile<w, kDefaultShape>();
+  SegLayout L;
+  L.max_large = std::min(nseg, n / (tile + 1) + 1);
+  L.max_tiles = n / tile + L.max_large + 1;
+  L.hist_bytes = L.max_large * Tr::kPasses * kRadix * 4;
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    const size_t at = off;
+    off += align_up(bytes, 256);
+    return at;
+  };
+  L.state_off = take(sizeof(RadixState));
+  L.hdr_off = take(sizeof(SegPlanHeader));
+  L.small_off = take(nseg * 4);
+  L.medium_off = take(nseg * 4);
+  L.large_off = take(nseg * 4);
+  L.prefix_off = take((nseg + 1) * 4);
+  L.hist_off = take(L.hist_bytes);
+  L.bucket_off = take(L.hist_bytes);
+  L.lb0_off = take(L.max_tiles * kRadix * 4);
+  L.lb1_off = take(L.max_tiles * kRadix * 4);
+  L.keys_off = take(n * sizeof(typename Tr::Bits));
+  L.total = off;
+  return L;
+}
+
+template <class Tr>
+cudaError_t segmented_sort_typed(typename Tr::Bits* keys, size_t n, const uint64_t* d_offsets, size_t nseg,
+                                 void* temp, size_t temp_bytes, cudaStream_t stream, uint32_t* d_status,
+                                 LaunchRecorder* rec) {
+  using Bits = typename Tr::Bits;
+  using Shape = OnesweepShape<sizeof(Bits), kDefaultShape>;
+  using Smem = OnesweepSmem<Tr, Shape::kBlock, Shape::kItems, Shape::kChains>;
+  constexpr uint32_t kTile = uint32_t(shape_tile<int(sizeof(Bits)), kDefaultShape>());
+  if (n == 0 || nseg == 0) return cudaSuccess;
+  if (n >= (size_t(1) << 32) || nseg >= (size_t(1) << 32) - 1) return cudaErrorInvalidValue;
+  const SegLayout L = seg_layout<Tr>(n, nseg);
+  if (temp == nullptr || temp_bytes < L.total) return cudaErrorInvalidValue;
+  char* tb = static_cast<char*>(temp);
+  RadixState* st = reinterpret_cast<RadixState*>(tb + L.state_off);
+  SegPlanHeader* hdr = reinterpret_cast<SegPlanHeader*>(tb + L.hdr_off);
+  uint32_t* small_ids = reinterpret_cast<uint32_t*>(tb + L.small_off);
+  uint32_t* medium_ids = reinterpret_cast<uint32_t*>(tb + L.medium_off);
+  uint32_t* large_ids = reinterpret_cast<uint32_t*>(tb + L.large_off);
+  uint32_t* prefix = reinterpret_cast<uint32_t*>(tb + L.prefix_off);
+  uint32_t* hist = reinterpret_cast<uint32_t*>(tb + L.hist_off);
+  uint32_t* bucket = reinterpret_cast<uint32_t*>(tb + L.bucket_off);
+  uint32_t* lb[2] = {reinterpret_cast<uint32_t*>(tb + L.lb0_off), reinterpret_cast<uint32_t*>(tb + L.lb1_off)};
+  Bits* tmp = reinterpret_cast<Bits*>(tb + L.keys_off);
+  const unsigned long long* offs = reinterpret_cast<const unsigned long long*>(d_offsets);
+
+  cudaError_t e = cudaMemsetAsync(tb, 0, L.small_off, stream);  // RadixState + plan header
+  if (e == cudaSuccess && L.hist_bytes) e = cudaMemsetAsync(hist, 0, L.hist_bytes, stream);
+  if (e != cudaSuccess) return e;
+  e = launch_kernel(rec, "seg_classify", seg_classify_kernel<1024>, dim3(1), dim3(1024), 0, stream, offs,
+                    uint32_t(nseg), (unsigned long long)n, kTile, kTile, hdr, small_ids, medium_ids, large_ids,
+                    prefix, d_status);
+  if (e != cudaSuccess) return e;
+
+  const int sms = device_sm_count();
+  {
+    auto kernel = seg_small_medium_kernel<Tr, Shape::kBlock, Shape::kItems, Shape::kMinBlocks, Shape::kChains, 2>;
+    static std::once_flag once;
+    std::call_once(once, [&] {
+      cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(Smem)));
+    });
+    e = launch_kernel(rec, "seg_small_medium", kernel, dim3(unsigned(sms)), dim3(Shape::kBlock), sizeof(Smem),
+                      stream, keys, offs, hdr, static_cast<const uint32_t*>(small_ids),
+                      static_cast<const uint32_t*>(medium_ids));
+    if (e != cudaSuccess) return e;
+  }
+  SegLarge sg{offs, large_ids, prefix, hdr->counts, bucket};
+  e = launch_kernel(rec, "seg_histogram", seg_histogram_kernel<Tr, 256>, dim3(unsigned(sms * 4)), dim3(256), 0,
+                    stream, static_cast<const Bits*>(keys), sg, kTile, hist, lb[0]);
+  if (e != cudaSuccess) return e;
+  e = launch_kernel(rec, "seg_scan", seg_scan_kernel<Tr::kPasses>, dim3(unsigned(sms * 4)), dim3(kRadix), 0, stream,
+                    static_cast<const uint32_t*>(hdr->counts), static_cast<const uint32_t*>(hist), bucket);
+  if (e != cudaSuccess) return e;
+  {
+    auto kernel = radix_onesweep_kernel<Tr, Shape::kBlock, Shape::kItems, Shape::kMinBlocks, Shape::kChains,
+                                        uint32_t, 2, true>;
+    static std::once_flag once;
+    std::call_once(once, [&] {
+      cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(Smem)));
+    });
+    for (int p = 0; p < Tr::kPasses; ++p) {
+      uint32_t* next = (p + 1 < Tr::kPasses) ? lb[(p + 1) & 1] : nullptr;
+      e = launch_kernel(rec, "seg_onesweep", kernel, dim3(unsigned(sms)), dim3(Shape::kBlock), sizeof(Smem), stream,
+                        keys, tmp, st, lb[p & 1], next, uint32_t(n), 0u, p, 1, sg);
+      if (e != cudaSuccess) return e;
+    }
+  }
+  // Passes are never skipped here (an even number ran): only the status report.
+  return launch_kernel(rec, "radix_finalize", radix_finalize_kernel<Tr>, dim3(1), dim3(256), 0, stream, keys,
+                       static_cast<const Bits*>(tmp), static_cast<const RadixState*>(st), 0u, d_status);
+}
+
 }  // namespace
 
 size_t radix_sort_temp_bytes(int dtype, size_t n) {
@@ -661,6 +1117,24 @@ int radix_sort_launches(int dtype, size_t n) {
   if (n == 0) return 0;
   const size_t w = dtype_bytes(dtype);
   return int(3 + w);  // histogram + scan + one onesweep per 8-bit digit + finalize
+}
+
+size_t segmented_sort_temp_bytes(int dtype, size_t n, size_t num_segments) {
+  size_t bytes = 0;
+  dispatch_dtype(dtype, [&](auto tr) { bytes = seg_layout<decltype(tr)>(n, num_segments).total; });
+  return bytes;
+}
+
+cudaError_t segmented_sort(int dtype, void* d_keys, size_t n, const uint64_t* d_offsets, size_t num_segments,
+                           void* d_temp, size_t temp_bytes, cudaStream_t stream, uint32_t* d_status,
+                           LaunchRecorder* rec) {
+  cudaError_t result = cudaErrorInvalidValue;
+  dispatch_dtype(dtype, [&](auto tr) {
+    using Tr = decltype(tr);
+    result = segmented_sort_typed<Tr>(static_cast<typename Tr::Bits*>(d_keys), n, d_offsets, num_segments, d_temp,
+                                      temp_bytes, stream, d_status, rec);
+  });
+  return result;
 }
 
 cudaError_t radix_sort(int dtype, void* d_keys, size_t n, void* d_temp, size_t temp_bytes, cudaStream_t stream,

@@ -92,6 +92,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "mgs_merge_device": ([c_void, c_int, c_void, c_size, c_void, c_size, c_void, c_void, c_size, c_void], c_int),
         "mgs_kway_merge_device": ([c_void, c_int, ctypes.POINTER(c_void), ctypes.POINTER(c_size), c_int, c_void,
                                    c_void, c_size, c_void], c_int),
+        "mgs_segmented_sort_temp_bytes": ([c_int, c_size, c_size, ctypes.POINTER(c_size)], c_int),
+        "mgs_segmented_sort_device": ([c_void, c_int, c_void, c_size, c_void, c_size, c_void, c_size, c_void], c_int),
         "mgs_gowanlock_sort": ([c_void, c_int, c_void, c_size, c_size, c_size, c_size, c_int], c_int),
         "mgs_ctx_phase_seconds": ([c_void, ctypes.c_char_p, ctypes.POINTER(ctypes.c_double)], c_int),
     }
@@ -258,6 +260,21 @@ class Context:
         _check(self._lib.mgs_kway_merge_device(self.handle, dtype_code(dtype), rp, lp, k, ctypes.c_void_p(d_out),
                                                ctypes.c_void_p(d_temp or None), int(temp_bytes),
                                                ctypes.c_void_p(stream or None)))
+
+    # --- batched segmented sort ---
+    @staticmethod
+    def segmented_sort_temp_bytes(dtype, n: int, num_segments: int) -> int:
+        lib = load_library()
+        b = ctypes.c_size_t()
+        _check(lib.mgs_segmented_sort_temp_bytes(dtype_code(dtype), int(n), int(num_segments), ctypes.byref(b)))
+        return b.value
+
+    def segmented_sort_device(self, d_keys: int, n: int, d_offsets: int, num_segments: int, dtype, d_temp: int = 0,
+                              temp_bytes: int = 0, stream: int = 0) -> None:
+        _check(self._lib.mgs_segmented_sort_device(self.handle, dtype_code(dtype), ctypes.c_void_p(d_keys), int(n),
+                                                   ctypes.c_void_p(d_offsets), int(num_segments),
+                                                   ctypes.c_void_p(d_temp or None), int(temp_bytes),
+                                                   ctypes.c_void_p(stream or None)))
 
     # --- GowanlockSort with one GPU: out-of-core chunk pipeline ---
     def gowanlock_sort(self, keys: np.ndarray, chunk_size: int = 0, merge_group_size: int = 0, num_buffers: int = 2,
