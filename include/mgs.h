@@ -200,6 +200,46 @@ int mgs_gowanlock_sort(mgs_ctx* ctx, int dtype, void* h_keys, size_t n, size_t c
  * "sort_phase" (chunk sorting and merging), "merge_phase", "memory_deallocation". */
 int mgs_ctx_phase_seconds(mgs_ctx* ctx, const char* phase, double* seconds);
 
+/* ---- serving loop (no counterpart in the reference) -------------------------
+ * Sort requests of mixed sizes and key types, submitted from any thread, are
+ * batched onto one GPU by a dispatcher thread (continuous batching): device
+ * memory is reserved once as num_slots resident slots (as many as
+ * device_budget_bytes admits); a queued request starts when a slot is free
+ * (admission by free HBM); a small request (<= coalesce_keys) opens a batch
+ * that every other queued small request of the same key type joins while the
+ * slot has room, sorted by one segmented-sort launch sequence; larger requests
+ * run alone. Each slot has its own stream, so batches overlap on the device.
+ * Requests are sorted in place in the caller's host buffer (pinned for full
+ * speed), which must stay valid until mgs_server_wait reports it finished.
+ * coalesce_keys = 0 and num_slots = 1 give the plain one-request-per-launch
+ * form. Zero config fields take defaults: num_slots 4, slot_keys 2^26 (keys of
+ * up to 8 bytes per slot), coalesce_keys 0 (no coalescing), max_batch_requests
+ * 4096, device_budget_bytes 80% of free device memory. */
+typedef struct mgs_server mgs_server;
+typedef struct mgs_server_config {
+  int device;
+  int num_slots;
+  size_t slot_keys;
+  size_t coalesce_keys;
+  size_t max_batch_requests;
+  size_t device_budget_bytes;
+} mgs_server_config;
+typedef struct mgs_server_stats {
+  uint64_t submitted, completed, rejected, cancelled, batches, keys, kernel_launches;
+  int num_slots;
+  double p50_us, p99_us, mean_us, max_us; /* latency: completion - submission */
+  double busy_s;                          /* first submission to last completion */
+} mgs_server_stats;
+int mgs_server_create(const mgs_server_config* config, mgs_server** out);
+int mgs_server_destroy(mgs_server* server); /* finishes queued and running requests first */
+int mgs_server_submit(mgs_server* server, int dtype, void* h_keys, size_t n, uint64_t* request_id);
+/* Waits for a request (timeout_ms < 0: no limit); MGS_ERR_TIMEOUT if it is still
+ * running. *request_status: MGS_OK, MGS_ERR_CANCELLED or the failure. A request
+ * is forgotten once a wait has reported it finished. */
+int mgs_server_wait(mgs_server* server, uint64_t request_id, int timeout_ms, int* request_status);
+int mgs_server_cancel(mgs_server* server, uint64_t request_id); /* queued requests only, else MGS_ERR_BUSY */
+int mgs_server_stats_get(mgs_server* server, mgs_server_stats* out, int reset);
+
 /* ---- DataGenerator::ComputeDistribution<T> (src/data_generator.cuh:18-36) ----
  * Fills the host buffer out[0..n) exactly as the reference generator does for
  * the reference's distributions: "uniform", "normal", "zero", "staggered",

@@ -97,6 +97,9 @@ void ref_zero(T* out, size_t n) {
   for (size_t i = 0; i < n; ++i) out[i] = 0;
 }
 
+// The bucket bounds below keep the reference's expression `num_buckets > upper`
+// (size_t against T) and its implicit conversions, on purpose.
+#pragma GCC diagnostic ignored "-Wsign-compare"
 // src/data_generator.cuh:81-115. Ten buckets; each bucket is uniform over a
 // window of width 10 below a random upper bound; the tail that does not fill a
 // bucket uses a separate generator seeded with seed + 128.

@@ -49,6 +49,20 @@ class MgsError(RuntimeError):
         self.code = code
 
 
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("num_slots", ctypes.c_int), ("slot_keys", ctypes.c_size_t),
+                ("coalesce_keys", ctypes.c_size_t), ("max_batch_requests", ctypes.c_size_t),
+                ("device_budget_bytes", ctypes.c_size_t)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64), ("rejected", ctypes.c_uint64),
+                ("cancelled", ctypes.c_uint64), ("batches", ctypes.c_uint64), ("keys", ctypes.c_uint64),
+                ("kernel_launches", ctypes.c_uint64), ("num_slots", ctypes.c_int), ("p50_us", ctypes.c_double),
+                ("p99_us", ctypes.c_double), ("mean_us", ctypes.c_double), ("max_us", ctypes.c_double),
+                ("busy_s", ctypes.c_double)]
+
+
 class KernelTime(ctypes.Structure):
     _fields_ = [("name", ctypes.c_char * 48), ("launches", ctypes.c_uint64), ("total_ms", ctypes.c_double)]
 
@@ -94,6 +108,12 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
                                    c_void, c_size, c_void], c_int),
         "mgs_segmented_sort_temp_bytes": ([c_int, c_size, c_size, ctypes.POINTER(c_size)], c_int),
         "mgs_segmented_sort_device": ([c_void, c_int, c_void, c_size, c_void, c_size, c_void, c_size, c_void], c_int),
+        "mgs_server_create": ([ctypes.POINTER(ServerConfig), ctypes.POINTER(c_void)], c_int),
+        "mgs_server_destroy": ([c_void], c_int),
+        "mgs_server_submit": ([c_void, c_int, c_void, c_size, ctypes.POINTER(ctypes.c_uint64)], c_int),
+        "mgs_server_wait": ([c_void, ctypes.c_uint64, c_int, ctypes.POINTER(c_int)], c_int),
+        "mgs_server_cancel": ([c_void, ctypes.c_uint64], c_int),
+        "mgs_server_stats_get": ([c_void, ctypes.POINTER(ServerStats), c_int], c_int),
         "mgs_gowanlock_sort": ([c_void, c_int, c_void, c_size, c_size, c_size, c_size, c_int], c_int),
         "mgs_ctx_phase_seconds": ([c_void, ctypes.c_char_p, ctypes.POINTER(ctypes.c_double)], c_int),
     }
@@ -312,3 +332,44 @@ class Context:
         v = ctypes.c_uint64()
         _check(self._lib.mgs_ctx_launch_count(self.handle, ctypes.byref(v), 1 if reset else 0))
         return int(v.value)
+
+
+class Server:
+    """The serving loop (mgs_server_*): continuous batching of sort requests on one GPU."""
+
+    def __init__(self, device: int = 0, num_slots: int = 4, slot_keys: int = 0, coalesce_keys: int = 1 << 20,
+                 max_batch_requests: int = 0, device_budget_bytes: int = 0):
+        self._lib = load_library()
+        cfg = ServerConfig(device, num_slots, slot_keys, coalesce_keys, max_batch_requests, device_budget_bytes)
+        h = ctypes.c_void_p()
+        _check(self._lib.mgs_server_create(ctypes.byref(cfg), ctypes.byref(h)))
+        self.handle = h
+        self._keep = {}
+        self._fin = weakref.finalize(self, self._lib.mgs_server_destroy, h)
+
+    def close(self) -> None:
+        if self._fin.alive:
+            self._fin()
+
+    def submit(self, keys: np.ndarray) -> int:
+        """Queues keys (sorted in place); returns the request id. Keep `keys` alive until wait()."""
+        assert keys.flags.c_contiguous
+        rid = ctypes.c_uint64()
+        _check(self._lib.mgs_server_submit(self.handle, dtype_code(keys.dtype), keys.ctypes.data_as(ctypes.c_void_p),
+                                           keys.size, ctypes.byref(rid)))
+        self._keep[rid.value] = keys
+        return rid.value
+
+    def wait(self, request_id: int, timeout_ms: int = -1) -> int:
+        st = ctypes.c_int()
+        _check(self._lib.mgs_server_wait(self.handle, request_id, timeout_ms, ctypes.byref(st)))
+        self._keep.pop(request_id, None)
+        return st.value
+
+    def cancel(self, request_id: int) -> None:
+        _check(self._lib.mgs_server_cancel(self.handle, request_id))
+
+    def stats(self, reset: bool = False) -> dict:
+        st = ServerStats()
+        _check(self._lib.mgs_server_stats_get(self.handle, ctypes.byref(st), 1 if reset else 0))
+        return {name: getattr(st, name) for name, _ in ServerStats._fields_}

@@ -1,0 +1,111 @@
+"""The serving loop: mixed request sizes and key types from several threads,
+continuous batching with coalescing; every result equals the oracle and is the
+same alone and in the mix; cancellation, admission limits and statistics."""
+import threading
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+TYPES = ["u32", "i32", "f32", "u64"]
+
+
+def make_requests(mgs, seed, count, max_log2=17):
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        dtype = TYPES[rng.integers(0, len(TYPES))]
+        n = int(2 ** rng.uniform(0, max_log2))
+        dist = "full-uniform-specials" if dtype == "f32" else "full-uniform"
+        a = mgs.generate(dtype, dist, seed * 1000 + i, n)
+        h = mgs.host_empty(n, a.dtype)
+        h[:] = a
+        out.append((a, h))
+    return out
+
+
+def test_mixed_requests_match_oracle_and_alone(mgs, orc):
+    reqs = make_requests(mgs, 1, 300)
+    srv = mgs.Server(0, num_slots=4, slot_keys=1 << 22, coalesce_keys=1 << 14)
+    try:
+        ids = [srv.submit(h) for _, h in reqs]
+        assert all(srv.wait(i) == mgs.MGS_OK for i in ids)
+        for a, h in reqs:
+            assert h.tobytes() == orc.sort(a).tobytes()
+        st = srv.stats()
+        assert st["completed"] == len(reqs) and st["batches"] < len(reqs)  # small requests were coalesced
+        assert st["p99_us"] >= st["p50_us"] > 0
+        # the same requests one at a time give the same bytes
+        for a, h_mix in reqs[:40]:
+            h = mgs.host_empty(a.size, a.dtype)
+            h[:] = a
+            assert srv.wait(srv.submit(h)) == mgs.MGS_OK
+            assert h.tobytes() == h_mix.tobytes()
+    finally:
+        srv.close()
+
+
+def test_concurrent_submitters(mgs, orc):
+    srv = mgs.Server(0, num_slots=3, slot_keys=1 << 21, coalesce_keys=1 << 12)
+    errors = []
+
+    def worker(seed):
+        try:
+            reqs = make_requests(mgs, seed, 60, max_log2=15)
+            ids = [srv.submit(h) for _, h in reqs]
+            for i in ids:
+                assert srv.wait(i) == mgs.MGS_OK
+            for a, h in reqs:
+                assert h.tobytes() == orc.sort(a).tobytes()
+        except Exception as e:  # pragma: no cover - reported below
+            errors.append(e)
+
+    threads = [threading.Thread(target=worker, args=(s,)) for s in range(10, 14)]
+    [t.start() for t in threads]
+    [t.join() for t in threads]
+    srv.close()
+    assert not errors, errors
+
+
+def test_plain_form_one_request_per_launch(mgs, orc):
+    reqs = make_requests(mgs, 3, 40, max_log2=14)
+    srv = mgs.Server(0, num_slots=1, slot_keys=1 << 20, coalesce_keys=0)
+    try:
+        ids = [srv.submit(h) for _, h in reqs]
+        assert all(srv.wait(i) == mgs.MGS_OK for i in ids)
+        for a, h in reqs:
+            assert h.tobytes() == orc.sort(a).tobytes()
+        st = srv.stats()
+        assert st["batches"] == sum(1 for a, _ in reqs if a.size > 1)
+    finally:
+        srv.close()
+
+
+def test_limits_cancel_and_timeout(mgs):
+    srv = mgs.Server(0, num_slots=1, slot_keys=1 << 16, coalesce_keys=0)
+    try:
+        big = mgs.host_empty((1 << 16) + 1, np.uint64)
+        with pytest.raises(mgs.MgsError) as e:
+            srv.submit(big)
+        assert e.value.code == mgs.MGS_ERR_INVALID
+        # keep the single slot busy, then cancel a queued request
+        keys = [mgs.host_empty(1 << 16, np.uint32) for _ in range(20)]
+        for k in keys:
+            k[:] = np.arange(k.size, 0, -1, dtype=np.uint32)
+        ids = [srv.submit(k) for k in keys]
+        cancelled = 0
+        for i in reversed(ids):
+            try:
+                srv.cancel(i)
+                cancelled += 1
+            except mgs.MgsError as err:
+                assert err.code == mgs.MGS_ERR_BUSY
+        statuses = [srv.wait(i) for i in ids]
+        assert statuses.count(mgs.MGS_ERR_CANCELLED) == cancelled >= 1
+        for k, s in zip(keys, statuses):
+            if s == mgs.MGS_OK:
+                assert np.all(k[1:] >= k[:-1])
+        assert srv.stats()["cancelled"] == cancelled
+    finally:
+        srv.close()
