@@ -126,6 +126,141 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def zipf_segment_offsets(rng, nseg=100_000, total=1 << 28, s=1.2, max_len=1 << 22):
+    """Batched workload: nseg segments with Zipf(s) lengths in [1, max_len], rescaled to about `total`
+    keys (floor, at least 1 key), in random order."""
+    lengths = np.minimum(rng.zipf(s, nseg), max_len).astype(np.float64)
+    lengths = np.maximum(1, np.floor(lengths * (total / lengths.sum()))).astype(np.int64)
+    rng.shuffle(lengths)
+    offs = np.zeros(nseg + 1, dtype=np.int64)
+    offs[1:] = np.cumsum(lengths)
+    return offs
+
+
+def batched_bench(mgs, torch, ctx):
+    """Config 5a: one segmented-sort call over 10^5 Zipf(1.2) segments (~2^28 u32 keys) against the plain form,
+    one mgs_sort_device launch per segment, on the same device-resident keys."""
+    rng = np.random.default_rng(11)
+    offs = zipf_segment_offsets(rng)
+    n = int(offs[-1])
+    keys = mgs.generate("u32", "full-uniform", 5, n)
+    pristine = torch.from_numpy(keys.view(np.int32)).cuda()
+    work = torch.empty_like(pristine)
+    d_offs = torch.from_numpy(offs).cuda()
+    temp_bytes = mgs.Context.segmented_sort_temp_bytes("u32", n, offs.size - 1)
+    temp = torch.empty(temp_bytes, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.Stream()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    times = []
+    for i in range(4):
+        with torch.cuda.stream(stream):
+            work.copy_(pristine)
+            ev[0].record(stream)
+            ctx.segmented_sort_device(work.data_ptr(), n, d_offs.data_ptr(), offs.size - 1, "u32", temp.data_ptr(),
+                                      temp_bytes, stream.cuda_stream)
+            ev[1].record(stream)
+        stream.synchronize()
+        if i > 0:
+            times.append(ev[0].elapsed_time(ev[1]))
+    ctx.synchronize()
+    batched_ms = statistics.median(times)
+    # plain form: one sort launch sequence per segment, same stream
+    plain_temp = mgs.Context.sort_temp_bytes("u32", int(np.diff(offs).max()))
+    ptemp = torch.empty(plain_temp, dtype=torch.uint8, device="cuda")
+    base = work.data_ptr()
+    with torch.cuda.stream(stream):
+        work.copy_(pristine)
+        ev[0].record(stream)
+        for s in range(offs.size - 1):
+            length = int(offs[s + 1] - offs[s])
+            if length > 1:
+                ctx.sort_device(base + 4 * int(offs[s]), length, "u32", ptemp.data_ptr(), plain_temp,
+                                stream.cuda_stream)
+        ev[1].record(stream)
+    stream.synchronize()
+    ctx.synchronize()
+    plain_ms = ev[0].elapsed_time(ev[1])
+    lens = np.diff(offs)
+    return {"segments": int(offs.size - 1), "keys": n, "dtype": "u32",
+            "lengths": "Zipf(1.2) in [1, 2^22] rescaled to ~2^28 keys, random order",
+            "segments_le_256": int((lens <= 256).sum()), "segments_gt_16384": int((lens > 16384).sum()),
+            "batched_ms": batched_ms, "batched_keys_per_s": n / (batched_ms / 1e3),
+            "plain_ms": plain_ms, "plain_keys_per_s": n / (plain_ms / 1e3),
+            "speedup_vs_plain": plain_ms / batched_ms}
+
+
+def served_bench(mgs, budget_s=2.0):
+    """Config 5b: Poisson arrivals at 10/50/90% of each form's measured peak, request sizes log-uniform over
+    2^10..2^26 keys, key type uniform over u32/i32/f32/u64; coalescing server against the plain form
+    (one request per launch, one slot). Requests come from a pool of pinned buffers that a helper thread
+    refills from pristine copies after each completion."""
+    import threading
+    import queue as _queue
+    rng = np.random.default_rng(7)
+    types = ["u32", "i32", "f32", "u64"]
+    pool = []
+    for i, n in enumerate((2 ** rng.uniform(10, 26, 96)).astype(np.int64)):
+        a = mgs.generate(types[i % 4], "full-uniform", 100 + i, int(n))
+        h = mgs.host_empty(a.size, a.dtype)
+        h[:] = a
+        pool.append((a, h))
+    mean_keys = float(np.mean([a.size for a, _ in pool]))
+
+    def run(srv, rate, duration, max_requests):
+        free = _queue.Queue()
+        for i in range(len(pool)):
+            free.put(i)
+        done = _queue.Queue()
+
+        def reaper():
+            while True:
+                item = done.get()
+                if item is None:
+                    return
+                rid, i = item
+                assert srv.wait(rid) == mgs.MGS_OK
+                np.copyto(pool[i][1], pool[i][0])
+                free.put(i)
+
+        th = threading.Thread(target=reaper)
+        th.start()
+        srv.stats(reset=True)
+        t0 = time.perf_counter()
+        nxt = t0
+        sent = 0
+        while sent < max_requests and time.perf_counter() - t0 < duration:
+            if rate is not None:
+                nxt += rng.exponential(1.0 / rate)
+                while time.perf_counter() < nxt:
+                    pass
+            i = free.get()
+            done.put((srv.submit(pool[i][1]), i))
+            sent += 1
+        done.put(None)
+        th.join()
+        st = srv.stats()
+        return {"requests": st["completed"], "keys_per_s": st["keys"] / max(st["busy_s"], 1e-9),
+                "p50_ms": st["p50_us"] / 1e3, "p99_ms": st["p99_us"] / 1e3, "batches": st["batches"]}
+
+    out = {"request_keys": "log-uniform 2^10..2^26", "types": types, "pool": len(pool)}
+    forms = {"served": dict(num_slots=4, slot_keys=1 << 26, coalesce_keys=1 << 20),
+             "plain": dict(num_slots=1, slot_keys=1 << 26, coalesce_keys=0)}
+    for name, cfg in forms.items():
+        srv = mgs.Server(0, **cfg)
+        try:
+            peak = run(srv, None, budget_s, 4 * len(pool))
+            levels = []
+            for load in (0.1, 0.5, 0.9):
+                rate = load * peak["keys_per_s"] / mean_keys
+                r = run(srv, rate, budget_s, 10_000)
+                r["offered_load"] = load
+                levels.append(r)
+            out[name] = {"peak": peak, "loads": levels, "config": cfg}
+        finally:
+            srv.close()
+    return out
+
+
 def cpu_reference_sort(orc, base: np.ndarray, budget_s: float, max_reps: int):
     """Times the reference's gnu_parallel sort on copies of `base` (bounded)."""
     threads = orc.ref_num_procs()
@@ -183,6 +318,8 @@ def main():
     ap.add_argument("--n", type=int, default=N_KEYS)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched (segmented) measurement")
+    ap.add_argument("--no-served", action="store_true", help="skip the serving-loop measurement")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -283,12 +420,20 @@ def main():
         avg_ms = one[1] / one[0]
         alg_bytes = 2 * 4 * n  # each pass reads and writes every key
         achieved = alg_bytes / (avg_ms / 1e3) / 1e9
-        traffic = committed_traffic("radix_onesweep")
+        traffic = committed_traffic("radix_onesweep") if n == N_KEYS else None
         roof = {"bound": "hbm", "kernel": "radix_onesweep", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                 "traffic": traffic, "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_ms}
     sort_alg_bytes = 36 * n  # 4 passes x (read + write) + one histogram read, 4-byte keys
     sort_ms = total_ms / args.steps
+
+    batched = None
+    served = None
+    if rank == 0 and world == 1:
+        if not args.no_batched:
+            batched = batched_bench(mgs, torch, ctx)
+        if not args.no_served:
+            served = served_bench(mgs)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -316,6 +461,8 @@ def main():
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "keys/s", "h2d_bytes_per_step": 4 * n, "d2h_bytes_per_step": 4 * n,
                     "api": "mgs_sort_host (TanasicSort, one GPU)", "steps": len(e2e_times)},
+            "batched": batched,
+            "served": served,
             "gpu_launches": launches,
             "kernel_ms": {k: {"launches": v[0], "total_ms": v[1]} for k, v in ktimes.items()},
             "clocks": clocks.summary(),
