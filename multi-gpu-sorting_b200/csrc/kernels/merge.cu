@@ -464,11 +464,9 @@ cudaError_t kway_merge_typed(const void* const* runs_v, const size_t* lens, int 
   if (e != cudaSuccess) return e;
   auto kernel = tile_merge_kernel<Tr, Shape::kBlock, Shape::kItems>;
   const size_t smem = 2 * kTile * sizeof(Bits) + size_t(k) * 8 + size_t(2 * (k + 1)) * 4;
-  static std::once_flag once;
-  std::call_once(once, [&] {
-    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         int(2 * kTile * sizeof(Bits) + size_t(kMaxKwayRuns) * 8 + size_t(2 * (kMaxKwayRuns + 1)) * 4));
-  });
+  static SmemLimitOnce attr;
+  e = attr.ensure(kernel, 2 * kTile * sizeof(Bits) + size_t(kMaxKwayRuns) * 8 + size_t(2 * (kMaxKwayRuns + 1)) * 4);
+  if (e != cudaSuccess) return e;
   return launch_kernel(rec, k == 2 ? "merge_tiles" : "kway_merge_tiles", kernel, dim3(unsigned(L.num_tiles)),
                        dim3(Shape::kBlock), smem, stream, d_runs, k, static_cast<const u64*>(d_splits), out, u64(total));
 }

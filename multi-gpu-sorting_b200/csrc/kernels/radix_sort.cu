@@ -5,8 +5,10 @@
 //
 // Per sort of n keys of w bytes (P = w 8-bit digit passes):
 //   K1 radix_histogram : one streaming read of the keys builds all P digit
-//                        histograms at once (16-byte loads, shared-memory
-//                        sub-histograms) and clears the first look-back array.
+//                        histograms at once (16-byte loads; one shared-memory
+//                        copy of the histograms per lane, so that the atomics of
+//                        a warp never share a bank) and clears the first
+//                        look-back array.
 //   K1b radix_scan     : exclusive scan per pass -> global bucket starts; marks
 //                        passes whose digit is the same for every key (the
 //                        stable counting pass is then the identity and is skipped).
@@ -71,9 +73,19 @@ MGS_SHAPE(8, 6, 512, 20, 1, 1)
 constexpr int kNumShapes = 7;
 constexpr int kDefaultShape = 5;
 
-constexpr int kHistBlock = 256;
-constexpr int kHistSub = 4;
+constexpr int kHistBlock = 1024;
 constexpr int kHistUnroll = 4;
+// Histogram copies per CTA: counter (pass, digit, copy) lives at word
+// (pass * 256 + digit) * copies + copy, and lane l updates copy l % copies.
+// With 32 copies every atomic of a warp hits its own bank whatever the digits
+// are (random digits into one shared histogram cost about 3.5 bank wavefronts
+// per warp atomic, equal digits up to 32). 8-byte keys keep 16 copies so that
+// both widths use 128 KB.
+template <class Tr>
+struct HistCopies {
+  static constexpr int kCopies = Tr::kPasses <= 4 ? 32 : 16;
+  static constexpr size_t kSmemBytes = size_t(Tr::kPasses) * kRadix * kCopies * sizeof(uint32_t);
+};
 constexpr uint32_t kLookbackSpinLimit = 1u << 25;
 constexpr uint32_t kTmaWaitLimit = 1u << 24;
 constexpr int kLookahead = 8;  // predecessor statuses fetched per look-back round
@@ -117,26 +129,28 @@ __device__ __forceinline__ void unpack_v4<unsigned long long>(const uint4& q, un
 
 // ---------------------------------------------------------------- K1 --------
 template <class Tr>
-__global__ __launch_bounds__(kHistBlock) void radix_histogram_kernel(const typename Tr::Bits* __restrict__ keys,
+__global__ __launch_bounds__(kHistBlock, 1) void radix_histogram_kernel(const typename Tr::Bits* __restrict__ keys,
                                                                      uint32_t n, RadixState* __restrict__ st,
                                                                      uint4* __restrict__ lb0, size_t lb0_vecs) {
   using Bits = typename Tr::Bits;
   constexpr int P = Tr::kPasses;
+  constexpr int C = HistCopies<Tr>::kCopies;
+  constexpr int kWords = P * kRadix * C;
   constexpr int kPerVec = 16 / int(sizeof(Bits));
-  __shared__ uint32_t sh[kHistSub][P][kRadix];
-  uint32_t* shf = &sh[0][0][0];
-  for (int i = threadIdx.x; i < kHistSub * P * kRadix; i += kHistBlock) shf[i] = 0u;
+  extern __shared__ __align__(16) uint32_t hist_smem[];
+  for (int i = threadIdx.x; i < kWords / 4; i += kHistBlock)
+    reinterpret_cast<uint4*>(hist_smem)[i] = make_uint4(0u, 0u, 0u, 0u);
 
   const size_t gtid = size_t(blockIdx.x) * kHistBlock + threadIdx.x;
   const size_t gstride = size_t(gridDim.x) * kHistBlock;
   for (size_t i = gtid; i < lb0_vecs; i += gstride) lb0[i] = make_uint4(0u, 0u, 0u, 0u);
   __syncthreads();
 
-  uint32_t(*hs)[kRadix] = sh[(threadIdx.x >> 5) % kHistSub];
+  uint32_t* const copy = hist_smem + (threadIdx.x & (C - 1));
   auto count_key = [&](Bits k) {
     const Bits o = Tr::Ordered(k);
 #pragma unroll
-    for (int p = 0; p < P; ++p) atomicAdd(&hs[p][uint32_t(o >> (8 * p)) & 0xFFu], 1u);
+    for (int p = 0; p < P; ++p) atomicAdd(copy + (p * kRadix + (uint32_t(o >> (8 * p)) & 0xFFu)) * C, 1u);
   };
 
   const uintptr_t addr = reinterpret_cast<uintptr_t>(keys);
@@ -168,11 +182,15 @@ __global__ __launch_bounds__(kHistBlock) void radix_histogram_kernel(const typen
     for (int j = 0; j < kPerVec; ++j) count_key(k[j]);
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < P * kRadix; i += kHistBlock) {
-    uint32_t s = 0;
+  // Fold the copies: a warp reads 32 consecutive words (32 / C counters) and
+  // sums each counter's C copies with shuffles.
+  const int lane = threadIdx.x & 31;
+  for (int w0 = (threadIdx.x >> 5) * 32; w0 < kWords; w0 += kHistBlock) {
+    uint32_t c = hist_smem[w0 + lane];
 #pragma unroll
-    for (int sub = 0; sub < kHistSub; ++sub) s += shf[sub * P * kRadix + i];
-    if (s) atomicAdd(&st->counts[i / kRadix][i % kRadix], s);
+    for (int off = C / 2; off >= 1; off >>= 1) c += __shfl_xor_sync(0xFFFFFFFFu, c, off);
+    const int row = (w0 + lane) / C;
+    if ((lane & (C - 1)) == 0 && c != 0u) atomicAdd(&st->counts[row / kRadix][row % kRadix], c);
   }
 }
 
@@ -918,10 +936,12 @@ cudaError_t launch_onesweep_passes(typename Tr::Bits* keys, typename Tr::Bits* t
   using Smem = OnesweepSmem<Tr, Shape::kBlock, Shape::kItems, Shape::kChains>;
   auto kernel = radix_onesweep_kernel<Tr, Shape::kBlock, Shape::kItems, Shape::kMinBlocks, Shape::kChains, StatusT,
                                       MATCH, false>;
+  static SmemLimitOnce attr;
+  cudaError_t e = attr.ensure(kernel, sizeof(Smem));
+  if (e != cudaSuccess) return e;
   static std::once_flag once;
   static int ctas_per_sm = 1;
   std::call_once(once, [&] {
-    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(Smem)));
     int occ = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, Shape::kBlock, sizeof(Smem)) == cudaSuccess &&
         occ > 0)
@@ -932,9 +952,8 @@ cudaError_t launch_onesweep_passes(typename Tr::Bits* keys, typename Tr::Bits* t
   for (int p = 0; p < Tr::kPasses; ++p) {
     StatusT* cur = lb[p & 1];
     StatusT* next = (p + 1 < Tr::kPasses) ? lb[(p + 1) & 1] : nullptr;
-    cudaError_t e = launch_kernel(rec, "radix_onesweep", kernel, dim3(unsigned(grid)), dim3(Shape::kBlock),
-                                  sizeof(Smem), stream, keys, tmp, st, cur, next, n, uint32_t(L.num_tiles), p,
-                                  use_tma ? 1 : 0, SegLarge{});
+    e = launch_kernel(rec, "radix_onesweep", kernel, dim3(unsigned(grid)), dim3(Shape::kBlock), sizeof(Smem), stream,
+                      keys, tmp, st, cur, next, n, uint32_t(L.num_tiles), p, use_tma ? 1 : 0, SegLarge{});
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
@@ -977,10 +996,14 @@ cudaError_t radix_sort_typed(typename Tr::Bits* keys, size_t n, void* temp, size
   const int sms = device_sm_count();
   const size_t vecs = n * sizeof(Bits) / 16 + 1;
   const size_t want = (vecs + size_t(kHistBlock) * kHistUnroll - 1) / (size_t(kHistBlock) * kHistUnroll);
-  const unsigned hist_grid = unsigned(std::max<size_t>(1, std::min<size_t>(size_t(sms) * 4, want)));
+  const unsigned hist_grid = unsigned(std::max<size_t>(1, std::min<size_t>(size_t(sms), want)));
   const size_t lb0_vecs = L.num_tiles * kRadix * L.status_bytes / 16;
-  e = launch_kernel(rec, "radix_histogram", radix_histogram_kernel<Tr>, dim3(hist_grid), dim3(kHistBlock), 0,
-                    stream, keys, n32, st, reinterpret_cast<uint4*>(tb + L.lb0_off), lb0_vecs);
+  static SmemLimitOnce hist_attr;
+  e = hist_attr.ensure(radix_histogram_kernel<Tr>, HistCopies<Tr>::kSmemBytes);
+  if (e != cudaSuccess) return e;
+  e = launch_kernel(rec, "radix_histogram", radix_histogram_kernel<Tr>, dim3(hist_grid), dim3(kHistBlock),
+                    HistCopies<Tr>::kSmemBytes, stream, keys, n32, st, reinterpret_cast<uint4*>(tb + L.lb0_off),
+                    lb0_vecs);
   if (e != cudaSuccess) return e;
   e = launch_kernel(rec, "radix_scan", radix_scan_kernel, dim3(Tr::kPasses), dim3(kRadix), 0, stream, st, n32);
   if (e != cudaSuccess) return e;
@@ -1070,10 +1093,9 @@ cudaError_t segmented_sort_typed(typename Tr::Bits* keys, size_t n, const uint64
   const int sms = device_sm_count();
   {
     auto kernel = seg_small_medium_kernel<Tr, Shape::kBlock, Shape::kItems, Shape::kMinBlocks, Shape::kChains, 2>;
-    static std::once_flag once;
-    std::call_once(once, [&] {
-      cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(Smem)));
-    });
+    static SmemLimitOnce attr;
+    e = attr.ensure(kernel, sizeof(Smem));
+    if (e != cudaSuccess) return e;
     e = launch_kernel(rec, "seg_small_medium", kernel, dim3(unsigned(sms)), dim3(Shape::kBlock), sizeof(Smem),
                       stream, keys, offs, hdr, static_cast<const uint32_t*>(small_ids),
                       static_cast<const uint32_t*>(medium_ids));
@@ -1089,10 +1111,9 @@ cudaError_t segmented_sort_typed(typename Tr::Bits* keys, size_t n, const uint64
   {
     auto kernel = radix_onesweep_kernel<Tr, Shape::kBlock, Shape::kItems, Shape::kMinBlocks, Shape::kChains,
                                         uint32_t, 2, true>;
-    static std::once_flag once;
-    std::call_once(once, [&] {
-      cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(Smem)));
-    });
+    static SmemLimitOnce attr;
+    e = attr.ensure(kernel, sizeof(Smem));
+    if (e != cudaSuccess) return e;
     for (int p = 0; p < Tr::kPasses; ++p) {
       uint32_t* next = (p + 1 < Tr::kPasses) ? lb[(p + 1) & 1] : nullptr;
       e = launch_kernel(rec, "seg_onesweep", kernel, dim3(unsigned(sms)), dim3(Shape::kBlock), sizeof(Smem), stream,
