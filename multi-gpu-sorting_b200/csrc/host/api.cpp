@@ -14,6 +14,7 @@
 #include "../kernels/merge.cuh"
 #include "../kernels/radix_sort.cuh"
 #include "chunk_sort.h"
+#include "staged_sort.h"
 #include "context.h"
 #include "out_of_core.h"
 
@@ -264,6 +265,21 @@ int mgs_sort_host(mgs_ctx* ctx, int dtype, void* h_keys, size_t n) {
   if (n > kMaxDeviceSortKeys) return invalid("mgs_sort_host: n must be below 2^32");
   Context& c = ctx->impl;
   DeviceGuard g(c.device);
+  if (mgs::plan_staged(n, w).slabs > 1) {
+    // Copies overlapped with slab sorts and a windowed merge; needs room for
+    // two copies of the keys, else the plain path below runs.
+    cudaError_t e = mgs::staged_host_sort(c, dtype, h_keys, n);
+    if (e == cudaSuccess) {
+      uint32_t status = 0;
+      e = c.take_status(c.compute, &status);
+      if (e != cudaSuccess) return cuda_fail(e, "mgs_sort_host: synchronize");
+      int rc = status_to_code(status);
+      if (rc == MGS_OK) mgs::clear_last_error();
+      return rc;
+    }
+    if (e != cudaErrorMemoryAllocation) return cuda_fail(e, "mgs_sort_host: staged sort");
+    cudaGetLastError();
+  }
   const size_t bytes = n * w;
   const size_t keys_bytes = align256(bytes);
   const size_t temp = mgs::radix_sort_temp_bytes(dtype, n);

@@ -221,7 +221,7 @@ __global__ __launch_bounds__(128) void kway_partition_kernel(
 template <class Tr, int BLOCK, int ITEMS>
 __global__ __launch_bounds__(BLOCK) void tile_merge_kernel(const typename Tr::Bits* const* __restrict__ runs, int k,
                                                            const u64* __restrict__ splits,
-                                                           typename Tr::Bits* __restrict__ out, u64 total) {
+                                                           typename Tr::Bits* __restrict__ out, u64 total, u64 tile0) {
   using Bits = typename Tr::Bits;
   constexpr int kTile = BLOCK * ITEMS;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -233,7 +233,7 @@ __global__ __launch_bounds__(BLOCK) void tile_merge_kernel(const typename Tr::Bi
   __shared__ uint32_t scan_tmp[BLOCK / 32 + 1];
 
   const int tid = threadIdx.x;
-  const u64 j = blockIdx.x;
+  const u64 j = tile0 + blockIdx.x;
   const u64 d0 = j * u64(kTile);
   const uint32_t cnt = uint32_t(min(u64(kTile), total - d0));
 
@@ -401,7 +401,8 @@ KwayLayout kway_layout(int k, size_t total) {
 
 template <class Tr>
 cudaError_t kway_merge_typed(const void* const* runs_v, const size_t* lens, int k, void* out_v, void* temp,
-                             size_t temp_bytes, cudaStream_t stream, LaunchRecorder* rec) {
+                             size_t temp_bytes, size_t window_keys, const MergeWindowFn& on_window,
+                             cudaStream_t stream, LaunchRecorder* rec) {
   using Bits = typename Tr::Bits;
   using Shape = MergeShape<sizeof(Bits)>;
   constexpr u64 kTile = u64(Shape::kBlock) * Shape::kItems;
@@ -410,7 +411,11 @@ cudaError_t kway_merge_typed(const void* const* runs_v, const size_t* lens, int 
   for (int r = 0; r < k; ++r) total += lens[r];
   if (total == 0) return cudaSuccess;
   Bits* out = static_cast<Bits*>(out_v);
-  if (k == 1) return cudaMemcpyAsync(out, runs_v[0], lens[0] * sizeof(Bits), cudaMemcpyDeviceToDevice, stream);
+  if (k == 1) {
+    cudaError_t e = cudaMemcpyAsync(out, runs_v[0], lens[0] * sizeof(Bits), cudaMemcpyDeviceToDevice, stream);
+    if (e == cudaSuccess && on_window) e = on_window(0, total);
+    return e;
+  }
   const KwayLayout L = kway_layout<Tr>(k, total);
   if (temp == nullptr || temp_bytes < L.total) return cudaErrorInvalidValue;
   char* tb = static_cast<char*>(temp);
@@ -467,8 +472,22 @@ cudaError_t kway_merge_typed(const void* const* runs_v, const size_t* lens, int 
   static SmemLimitOnce attr;
   e = attr.ensure(kernel, 2 * kTile * sizeof(Bits) + size_t(kMaxKwayRuns) * 8 + size_t(2 * (kMaxKwayRuns + 1)) * 4);
   if (e != cudaSuccess) return e;
-  return launch_kernel(rec, k == 2 ? "merge_tiles" : "kway_merge_tiles", kernel, dim3(unsigned(L.num_tiles)),
-                       dim3(Shape::kBlock), smem, stream, d_runs, k, static_cast<const u64*>(d_splits), out, u64(total));
+  // Output tiles in windows of about window_keys keys (one window when 0).
+  const u64 per_window =
+      window_keys == 0 ? L.num_tiles : std::max<u64>(1, (u64(window_keys) + kTile - 1) / kTile);
+  for (u64 t0 = 0; t0 < L.num_tiles; t0 += per_window) {
+    const u64 t1 = std::min<u64>(L.num_tiles, t0 + per_window);
+    e = launch_kernel(rec, k == 2 ? "merge_tiles" : "kway_merge_tiles", kernel, dim3(unsigned(t1 - t0)),
+                      dim3(Shape::kBlock), smem, stream, d_runs, k, static_cast<const u64*>(d_splits), out, u64(total),
+                      t0);
+    if (e != cudaSuccess) return e;
+    if (on_window) {
+      const u64 first = t0 * kTile, last = std::min<u64>(u64(total), t1 * kTile);
+      e = on_window(size_t(first), size_t(last - first));
+      if (e != cudaSuccess) return e;
+    }
+  }
+  return cudaSuccess;
 }
 
 template <class Tr>
@@ -498,7 +517,18 @@ cudaError_t kway_merge(int dtype, const void* const* runs, const size_t* lens, i
                        size_t temp_bytes, cudaStream_t stream, LaunchRecorder* rec) {
   cudaError_t result = cudaErrorInvalidValue;
   dispatch_dtype(dtype, [&](auto tr) {
-    result = kway_merge_typed<decltype(tr)>(runs, lens, k, out, d_temp, temp_bytes, stream, rec);
+    result = kway_merge_typed<decltype(tr)>(runs, lens, k, out, d_temp, temp_bytes, 0, MergeWindowFn(), stream, rec);
+  });
+  return result;
+}
+
+cudaError_t kway_merge_windowed(int dtype, const void* const* runs, const size_t* lens, int k, void* out,
+                                void* d_temp, size_t temp_bytes, size_t window_keys, const MergeWindowFn& on_window,
+                                cudaStream_t stream, LaunchRecorder* rec) {
+  cudaError_t result = cudaErrorInvalidValue;
+  dispatch_dtype(dtype, [&](auto tr) {
+    result = kway_merge_typed<decltype(tr)>(runs, lens, k, out, d_temp, temp_bytes, window_keys, on_window, stream,
+                                            rec);
   });
   return result;
 }

@@ -9,6 +9,8 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#include <functional>
+
 #include "launch.cuh"
 
 namespace mgs {
@@ -33,5 +35,15 @@ size_t kway_merge_temp_bytes(int dtype, int k, size_t total);
 constexpr int kMaxKwayRuns = 1024;
 cudaError_t kway_merge(int dtype, const void* const* runs, const size_t* lens, int k, void* out, void* d_temp,
                        size_t temp_bytes, cudaStream_t stream, LaunchRecorder* rec);
+
+// As kway_merge, with the output merged in windows of about window_keys keys
+// (whole merge tiles), in output order: after the launch of each window is
+// enqueued on `stream`, on_window(first, count) is called with the window's
+// output range, so that the caller can hand it to another stream (a D2H copy
+// that overlaps the merge of the next window).
+using MergeWindowFn = std::function<cudaError_t(size_t first, size_t count)>;
+cudaError_t kway_merge_windowed(int dtype, const void* const* runs, const size_t* lens, int k, void* out,
+                                void* d_temp, size_t temp_bytes, size_t window_keys, const MergeWindowFn& on_window,
+                                cudaStream_t stream, LaunchRecorder* rec);
 
 }  // namespace mgs

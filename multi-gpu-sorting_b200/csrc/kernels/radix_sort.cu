@@ -14,8 +14,10 @@
 //                        stable counting pass is then the identity and is skipped).
 //   K2 radix_onesweep  : one launch per pass. Each CTA takes the next tile in
 //                        launch order from an atomic counter, stages it in shared
-//                        memory with a TMA bulk copy, ranks the keys by digit with
-//                        warp match (or ballots) and shared-memory counters,
+//                        memory with a TMA bulk copy, ranks the keys by digit
+//                        (peer groups from ballots for half of the items and
+//                        from shared-memory masks for the other half; per-warp
+//                        shared-memory counters),
 //                        publishes its digit counts, resolves its global offsets
 //                        by decoupled look-back over earlier tiles, and scatters
 //                        the tile from shared memory in digit order.
@@ -228,7 +230,16 @@ struct OnesweepSmem {
 //   MATCH 2: per-chain shared-memory masks: every lane ORs its bit into the
 //            mask of its digit, reads the mask back, and the last lane of each
 //            group clears it (masks alternate between two arrays per item).
+//   MATCH 3: ballots for half of the items (alternate items, or chain 0 of two),
+//            shared-memory masks for the rest, so that the integer-ALU work of
+//            one item overlaps the shared-memory latency of the next.
+//   MATCH 4: ballots for every fourth item, shared-memory masks otherwise.
 // `ok` separates padding lanes of a partial tile (their digit is 256 + lane).
+template <int MATCH, int CHAINS>
+__device__ __forceinline__ constexpr bool rank_by_ballot(int h, int j) {
+  return MATCH == 1 || (MATCH == 3 && (CHAINS == 1 ? (j & 1) == 0 : h == 0)) || (MATCH == 4 && (j & 3) == 0);
+}
+
 template <int MATCH, bool FULL>
 __device__ __forceinline__ uint32_t digit_peers(uint32_t d, bool ok, uint32_t* mm, int lane) {
   if (MATCH == 0) {
@@ -335,13 +346,15 @@ __device__ __forceinline__ bool rank_tile(OnesweepSmem<Tr, BLOCK, ITEMS, CHAINS>
       cc[h] = sm.ccount + (warp * CHAINS + h) * kRadix;
       mm[h] = sm.masks + (warp * CHAINS + h) * 2 * kRadix + (j & 1) * kRadix;
     }
-    if (MATCH == 2) {
+    if (MATCH >= 2) {
 #pragma unroll
       for (int h = 0; h < CHAINS; ++h)
-        if (ok[h]) atomicOr(&mm[h][d[h]], 1u << lane);
+        if (!rank_by_ballot<MATCH, CHAINS>(h, j) && ok[h]) atomicOr(&mm[h][d[h]], 1u << lane);
       __syncwarp();
 #pragma unroll
-      for (int h = 0; h < CHAINS; ++h) peers[h] = ok[h] ? mm[h][d[h]] : (1u << lane);
+      for (int h = 0; h < CHAINS; ++h)
+        peers[h] = rank_by_ballot<MATCH, CHAINS>(h, j) ? digit_peers<1, FULL>(d[h], ok[h], mm[h], lane)
+                                                         : (ok[h] ? mm[h][d[h]] : (1u << lane));
     } else {
 #pragma unroll
       for (int h = 0; h < CHAINS; ++h) peers[h] = digit_peers<MATCH, FULL>(d[h], ok[h], mm[h], lane);
@@ -353,10 +366,12 @@ __device__ __forceinline__ bool rank_tile(OnesweepSmem<Tr, BLOCK, ITEMS, CHAINS>
     for (int h = 0; h < CHAINS; ++h) {
       if (ok[h] && (peers[h] & lmask_gt) == 0) {
         cc[h][d[h]] = pos[h] + 1u;  // the last lane of each peer group advances the counter
-        if (MATCH == 2) mm[h][d[h]] = 0u;
+        if (MATCH >= 2 && !rank_by_ballot<MATCH, CHAINS>(h, j)) mm[h][d[h]] = 0u;
       }
     }
-    __syncwarp();
+    // With shared-memory masks the next item's first __syncwarp orders these
+    // counter updates before its counter reads; ballots and match need one here.
+    if (MATCH < 2) __syncwarp();
 #pragma unroll
     for (int h = 0; h < CHAINS; ++h)
       if (ok[h] && pos[h] < uint32_t(kTile)) dst[pos[h]] = key[h * kPerChain + j];
@@ -525,7 +540,7 @@ __global__ __launch_bounds__(BLOCK, MINB) void radix_onesweep_kernel(typename Tr
   // processed and the look-back makes progress.
   static_assert(sizeof(TileSpan<Tr>) <= sizeof(sm.span[0]), "span slot");
   TileSpan<Tr>* spans = reinterpret_cast<TileSpan<Tr>*>(sm.span);
-  if (MATCH == 2)
+  if (MATCH >= 2)
     for (int i = tid; i < kChains * 2 * kRadix; i += BLOCK) sm.masks[i] = 0u;
   if (tid == 0) {
     mbar_init(&sm.bar[0], 1);
@@ -892,7 +907,7 @@ int onesweep_shape() {
 int rank_mode() {
   static int mode = [] {
     const char* e = getenv("MGS_RANK_MODE");
-    return (e && e[0] >= '0' && e[0] <= '2') ? e[0] - '0' : 2;
+    return (e && e[0] >= '0' && e[0] <= '4') ? e[0] - '0' : 3;
   }();
   return mode;
 }
@@ -964,8 +979,17 @@ cudaError_t launch_onesweep_variant(typename Tr::Bits* keys, typename Tr::Bits* 
                                     const RadixLayout& L, uint32_t n, bool use_tma, cudaStream_t stream,
                                     LaunchRecorder* rec) {
 #define MGS_LAUNCH(S, M) launch_onesweep_passes<Tr, S, StatusT, M>(keys, tmp, st, tbase, L, n, use_tma, stream, rec)
-  if (rank_mode() == 1) return MGS_LAUNCH(kDefaultShape, 1);
-  if (rank_mode() == 0) return MGS_LAUNCH(kDefaultShape, 0);
+  const int mode = rank_mode();
+  if (mode == 0) return MGS_LAUNCH(kDefaultShape, 0);
+  if (mode == 1) return MGS_LAUNCH(kDefaultShape, 1);
+  if (mode == 4) return MGS_LAUNCH(kDefaultShape, 4);
+  if (mode == 3) {
+    switch (onesweep_shape()) {
+      case 4: return MGS_LAUNCH(4, 3);
+      case 6: return MGS_LAUNCH(6, 3);
+      default: return MGS_LAUNCH(kDefaultShape, 3);
+    }
+  }
   switch (onesweep_shape()) {
     case 0: return MGS_LAUNCH(0, 2);
     case 1: return MGS_LAUNCH(1, 2);
@@ -1092,7 +1116,7 @@ cudaError_t segmented_sort_typed(typename Tr::Bits* keys, size_t n, const uint64
 
   const int sms = device_sm_count();
   {
-    auto kernel = seg_small_medium_kernel<Tr, Shape::kBlock, Shape::kItems, Shape::kMinBlocks, Shape::kChains, 2>;
+    auto kernel = seg_small_medium_kernel<Tr, Shape::kBlock, Shape::kItems, Shape::kMinBlocks, Shape::kChains, 3>;
     static SmemLimitOnce attr;
     e = attr.ensure(kernel, sizeof(Smem));
     if (e != cudaSuccess) return e;
@@ -1110,7 +1134,7 @@ cudaError_t segmented_sort_typed(typename Tr::Bits* keys, size_t n, const uint64
   if (e != cudaSuccess) return e;
   {
     auto kernel = radix_onesweep_kernel<Tr, Shape::kBlock, Shape::kItems, Shape::kMinBlocks, Shape::kChains,
-                                        uint32_t, 2, true>;
+                                        uint32_t, 3, true>;
     static SmemLimitOnce attr;
     e = attr.ensure(kernel, sizeof(Smem));
     if (e != cudaSuccess) return e;
