@@ -276,11 +276,16 @@ __device__ __forceinline__ uint32_t digit_peers(uint32_t d, bool ok, uint32_t* m
 // onesweep publishes its look-back aggregate there). With ALLOW_SKIP, a digit
 // shared by every key makes the pass the identity: nothing is written and the
 // function returns true (block-uniform). sm.tile_start receives the exclusive
-// scan of the digit counts. The caller synchronizes before reading dst.
-template <class Tr, int BLOCK, int ITEMS, int CHAINS, int MATCH, bool FULL, bool ALLOW_SKIP, class OnCounts>
+// scan of the digit counts. between(count) runs on every thread once the
+// counts and tile starts are final and before the thread's warp ranks its keys
+// (count = the tile's count of digit tid for tid < 256): warps that do extra
+// work there rank later, while the other warps rank at once. The caller
+// synchronizes before reading dst.
+template <class Tr, int BLOCK, int ITEMS, int CHAINS, int MATCH, bool FULL, bool ALLOW_SKIP, class OnCounts,
+          class Between>
 __device__ __forceinline__ bool rank_tile(OnesweepSmem<Tr, BLOCK, ITEMS, CHAINS>& sm, const typename Tr::Bits* src,
                                           typename Tr::Bits* dst, uint32_t valid, int pass, uint32_t* tile_count_out,
-                                          OnCounts on_counts) {
+                                          OnCounts on_counts, Between between) {
   using Bits = typename Tr::Bits;
   constexpr int kTile = BLOCK * ITEMS;
   constexpr int kChains = (BLOCK / 32) * CHAINS;
@@ -326,6 +331,7 @@ __device__ __forceinline__ bool rank_tile(OnesweepSmem<Tr, BLOCK, ITEMS, CHAINS>
     }
   }
   __syncthreads();
+  between(tile_count);
 
   // Phase 2: stable rank within each chain (peer groups of equal digit, in lane
   // order); each key goes straight to its slot of the tile in digit order.
@@ -391,9 +397,9 @@ struct alignas(16) TileSpan {
   const uint32_t* bucket;        // 256 bucket starts of this pass within the segment
 };
 
-// One tile: rank in shared memory (publishing the tile's digit counts for the
-// look-back as soon as they are known), look back over the segment's earlier
-// tiles, scatter the digit runs.
+// One tile: count digits in shared memory (publishing the tile's counts for
+// the look-back as soon as they are known), look back over the segment's
+// earlier tiles while the other warps rank, scatter the digit runs.
 template <class Tr, int BLOCK, int ITEMS, int CHAINS, typename StatusT, int MATCH, bool FULL>
 __device__ __forceinline__ void onesweep_tile(OnesweepSmem<Tr, BLOCK, ITEMS, CHAINS>& sm, typename Tr::Bits* skeys,
                                               RadixState* __restrict__ st, StatusT* __restrict__ lb_cur,
@@ -401,55 +407,59 @@ __device__ __forceinline__ void onesweep_tile(OnesweepSmem<Tr, BLOCK, ITEMS, CHA
   using Bits = typename Tr::Bits;
   using LW = LookbackWord<StatusT>;
   const int tid = threadIdx.x;
+  // Decoupled look-back (one thread per digit: the first 256 threads) runs
+  // between the counting and the ranking of the tile: it walks back over
+  // earlier tiles of the segment, summing their aggregates until it meets an
+  // inclusive prefix, with the statuses of kLookahead predecessors fetched per
+  // round. With 512 threads the other eight warps rank their keys meanwhile, so
+  // the waits on other tiles overlap ranking.
   uint32_t tile_count = 0;
   rank_tile<Tr, BLOCK, ITEMS, CHAINS, MATCH, FULL, false>(
-      sm, skeys, skeys, valid, pass, &tile_count, [&](uint32_t count) {
+      sm, skeys, skeys, valid, pass, &tile_count,
+      [&](uint32_t count) {
         StatusT* slot = lb_cur + size_t(tile) * kRadix + tid;
         LW::store(slot, tile == span.first_tile ? (LW::kPrefix | StatusT(count)) : StatusT(count + 1u));
+      },
+      [&](uint32_t count) {
+        if (tid >= kRadix) return;
+        StatusT excl = 0;
+        if (tile > span.first_tile) {
+          const long long first = span.first_tile;
+          long long jt = static_cast<long long>(tile) - 1;
+          uint32_t spins = 0;
+          bool done = false;
+          while (!done && jt >= first) {
+            StatusT sv[kLookahead];
+#pragma unroll
+            for (int q = 0; q < kLookahead; ++q)
+              sv[q] = (jt - q >= first) ? LW::load(lb_cur + size_t(jt - q) * kRadix + tid) : (LW::kPrefix | StatusT(0));
+            int used = 0;
+#pragma unroll
+            for (int q = 0; q < kLookahead; ++q) {
+              if (done || used != q) continue;
+              const StatusT v = sv[q];
+              if (v == 0) continue;  // not published yet: poll it again
+              if (v & LW::kPrefix) {
+                excl += v & ~LW::kPrefix;
+                done = true;
+              } else {
+                excl += v - 1;
+                ++used;
+              }
+            }
+            jt -= used;
+            if (!done && used == 0) {
+              if (++spins >= kLookbackSpinLimit) {
+                atomicOr(&st->error, kStatusLookbackTimeout);
+                break;
+              }
+              if (spins > 8) __nanosleep(32);
+            }
+          }
+          LW::store(lb_cur + size_t(tile) * kRadix + tid, LW::kPrefix | (excl + count));
+        }
+        sm.gbase[tid] = span.bucket[tid] + uint32_t(excl) - sm.tile_start[tid];
       });
-
-  // Decoupled look-back: one thread per digit walks back over earlier tiles of
-  // the segment, summing their aggregates until it meets an inclusive prefix.
-  // Statuses of kLookahead predecessors are fetched per round.
-  if (tid < kRadix) {
-    StatusT excl = 0;
-    if (tile > span.first_tile) {
-      const long long first = span.first_tile;
-      long long jt = static_cast<long long>(tile) - 1;
-      uint32_t spins = 0;
-      bool done = false;
-      while (!done && jt >= first) {
-        StatusT sv[kLookahead];
-#pragma unroll
-        for (int q = 0; q < kLookahead; ++q)
-          sv[q] = (jt - q >= first) ? LW::load(lb_cur + size_t(jt - q) * kRadix + tid) : (LW::kPrefix | StatusT(0));
-        int used = 0;
-#pragma unroll
-        for (int q = 0; q < kLookahead; ++q) {
-          if (done || used != q) continue;
-          const StatusT v = sv[q];
-          if (v == 0) continue;  // not published yet: poll it again
-          if (v & LW::kPrefix) {
-            excl += v & ~LW::kPrefix;
-            done = true;
-          } else {
-            excl += v - 1;
-            ++used;
-          }
-        }
-        jt -= used;
-        if (!done && used == 0) {
-          if (++spins >= kLookbackSpinLimit) {
-            atomicOr(&st->error, kStatusLookbackTimeout);
-            break;
-          }
-          if (spins > 8) __nanosleep(32);
-        }
-      }
-      LW::store(lb_cur + size_t(tile) * kRadix + tid, LW::kPrefix | (excl + tile_count));
-    }
-    sm.gbase[tid] = span.bucket[tid] + uint32_t(excl) - sm.tile_start[tid];
-  }
   __syncthreads();
 
   // Phase 3: consecutive threads write consecutive positions of one digit run.
@@ -784,7 +794,7 @@ __global__ __launch_bounds__(BLOCK, MINB) void seg_small_medium_kernel(typename 
       for (int pass = 0; pass < Tr::kPasses; ++pass) {
         uint32_t tc;
         const bool skipped = rank_tile<Tr, BLOCK, ITEMS, CHAINS, MATCH, false, true>(
-            sm, sm.keys[cur], sm.keys[cur ^ 1], len, pass, &tc, [](uint32_t) {});
+            sm, sm.keys[cur], sm.keys[cur ^ 1], len, pass, &tc, [](uint32_t) {}, [](uint32_t) {});
         __syncthreads();
         if (!skipped) cur ^= 1;
       }
