@@ -261,6 +261,271 @@ def served_bench(mgs, budget_s=2.0):
     return out
 
 
+# ---------------------------------------------------------------- sweeps ----
+# `bench.py --sweep types|merge|ooc` measures the other workloads of the sort
+# API on one GPU and prints one JSON line per case instead of the headline line.
+
+SWEEP_DISTS = ["full-uniform", "normal0", "zipf", "sorted-full", "reverse-sorted-full", "nearly-sorted-swaps",
+               "all-equal"]
+
+
+def order_key(torch, t, dtype):
+    """int64 tensor whose signed order is the sort's order of the keys in t (same bits, int32/int64 storage):
+    unsigned for u32/u64, two's complement for i32, and for f32 the radix order (-0.0 equal to +0.0, NaN by
+    transformed bits)."""
+    if dtype == "u32":
+        return t.to(torch.int64) & 0xFFFFFFFF
+    if dtype == "i32":
+        return t.to(torch.int64)
+    if dtype == "u64":
+        return t ^ (-(1 << 63))
+    u = t.to(torch.int64) & 0xFFFFFFFF
+    u = torch.where(u == 0x80000000, torch.zeros_like(u), u)  # -0.0 -> +0.0
+    return torch.where(u >= 0x80000000, 0xFFFFFFFF - u, u + 0x80000000)
+
+
+def same_multiset_invariants(torch, a, b, dtype):
+    """Multiset invariants of two key tensors: sum and sum of squares (mod 2^64), the sum of a
+    multiplicative hash of every key (mod 2^64), and a 2^16-bin histogram of the order key's top bits."""
+    shift = 16 if a.element_size() == 4 else 48
+
+    def inv(t):
+        x = t.to(torch.int64)
+        h = x * -7046029254386353131  # 0x9E3779B97F4A7C15 as a signed 64-bit constant
+        top = (order_key(torch, t, dtype) >> shift) & 0xFFFF
+        return [x.sum(), (x * x).sum(), (h ^ (h >> 29)).sum(), torch.bincount(top, minlength=1 << 16)]
+
+    return all(torch.equal(u, v) for u, v in zip(inv(a), inv(b)))
+
+
+def verify_sorted_permutation(torch, out, src, dtype):
+    """On the device: out is ascending in the sort's order, holds the same multiset of bit patterns as src,
+    and (floats) keeps the input order of -0.0 and +0.0, which compare equal. Together these fix every
+    output byte."""
+    k = order_key(torch, out, dtype)
+    if not bool((k[1:] >= k[:-1]).all()):
+        return False
+    if out.numel() < (1 << 31) - 1:
+        if not torch.equal(torch.sort(out.view(-1))[0], torch.sort(src.view(-1))[0]):
+            return False
+    elif not same_multiset_invariants(torch, out, src, dtype):  # beyond torch.sort's element limit
+        return False
+    if dtype == "f32":
+        bits_in = src.to(torch.int64) & 0xFFFFFFFF
+        bits_out = out.to(torch.int64) & 0xFFFFFFFF
+        z_in = bits_in[(bits_in == 0) | (bits_in == 0x80000000)]
+        z_out = bits_out[(bits_out == 0) | (bits_out == 0x80000000)]
+        if not torch.equal(z_in, z_out):
+            return False
+    return True
+
+
+def sweep_types(mgs, torch, n, reps=3):
+    """Plain device sort of n keys of u32, i32, f32 and u64 over seven distributions (float arrays carry 0.1%
+    -0.0 and 0.1% NaN): keys/s and the fraction of the HBM roofline for the canonical n*w*(2P+1) bytes."""
+    ctx = mgs.Context(0)
+    peak, _ = measured_hbm_peak()
+    stream = torch.cuda.Stream()
+    for dtype in ["u32", "i32", "f32", "u64"]:
+        w = 8 if dtype == "u64" else 4
+        storage = (np.int64, torch.int64) if w == 8 else (np.int32, torch.int32)
+        temp_bytes = mgs.Context.sort_temp_bytes(dtype, n)
+        temp = torch.empty(temp_bytes, dtype=torch.uint8, device="cuda")
+        for dist in SWEEP_DISTS:
+            name = dist + ("-specials" if dtype == "f32" else "")
+            keys = mgs.generate(dtype, name, SEED, n)
+            src = torch.from_numpy(keys.view(storage[0])).cuda()
+            work = torch.empty_like(src)
+            times = []
+            for i in range(reps + 1):
+                with torch.cuda.stream(stream):
+                    work.copy_(src)
+                    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    a.record(stream)
+                    ctx.sort_device(work.data_ptr(), n, dtype, temp.data_ptr(), temp_bytes, stream.cuda_stream)
+                    b.record(stream)
+                stream.synchronize()
+                if i > 0:
+                    times.append(a.elapsed_time(b))
+            ok = verify_sorted_permutation(torch, work, src, dtype)
+            ms = statistics.median(times)
+            alg = n * w * (2 * w + 1)
+            print(json.dumps({"sweep": "types", "dtype": dtype, "distribution": name, "n": n, "ms": ms,
+                              "keys_per_s": n / (ms / 1e3), "hbm_alg_gbs": alg / (ms / 1e3) / 1e9,
+                              "roofline_frac": alg / (ms / 1e3) / 1e9 / peak, "reps": reps, "verified": ok}),
+                  flush=True)
+            del src, work
+        del temp
+    ctx.close()
+
+
+def dirichlet_lengths(rng, k, total):
+    w = rng.dirichlet(np.ones(k))
+    lens = np.floor(w * total).astype(np.int64)
+    lens[np.argmax(lens)] += total - int(lens.sum())
+    return [int(x) for x in lens]
+
+
+def sweep_merge(mgs, torch, n, reps=3):
+    """Chunked merge path (TanasicSort over g chunks of one GPU, g in 2, 4, 8) and the k-way merge of k in
+    2, 8, 32, 64 sorted runs with Dirichlet(1) lengths, n uint32 keys each."""
+    ctx = mgs.Context(0)
+    peak, _ = measured_hbm_peak()
+    g = torch.Generator(device="cuda")
+    g.manual_seed(SEED)
+    src = torch.randint(-2 ** 31, 2 ** 31 - 1, (n,), dtype=torch.int32, device="cuda", generator=g)
+    work = torch.empty_like(src)
+    for chunks in (2, 4, 8):
+        times = []
+        for i in range(reps + 1):
+            work.copy_(src)
+            torch.cuda.synchronize()
+            ctx.set_profiling(i > 0)
+            t0 = time.perf_counter()
+            ctx.tanasic_sort_device(work.data_ptr(), n, "u32", chunks)
+            dt = time.perf_counter() - t0
+            if i > 0:
+                times.append(dt)
+        kt = ctx.kernel_times()
+        ctx.set_profiling(False)
+        ok = verify_sorted_permutation(torch, work, src, "u32")
+        s = statistics.median(times)
+        merge_ms = sum(v[1] for k_, v in kt.items() if not k_.startswith("radix")) / reps
+        sort_ms = sum(v[1] for k_, v in kt.items() if k_.startswith("radix")) / reps
+        print(json.dumps({"sweep": "chunked_merge", "dtype": "u32", "n": n, "chunks": chunks, "s": s,
+                          "keys_per_s": n / s, "chunk_sort_kernel_ms": sort_ms, "merge_kernel_ms": merge_ms,
+                          "kernels": {k_: {"launches": v[0] // reps, "ms": v[1] / reps} for k_, v in kt.items()},
+                          "verified": ok}), flush=True)
+    del work
+    rng = np.random.default_rng(SEED)
+    out = torch.empty_like(src)
+    orc = None
+    for k in (2, 8, 32, 64):
+        lens = dirichlet_lengths(rng, k, n)
+        offs = np.concatenate([[0], np.cumsum(lens)])
+        runs = src.clone()
+        for r in range(k):
+            if lens[r] > 1:
+                ctx.sort_device(runs.data_ptr() + 4 * int(offs[r]), lens[r], "u32")
+        ctx.synchronize()
+        ptrs = [runs.data_ptr() + 4 * int(offs[r]) for r in range(k)]
+        temp_bytes = mgs.Context.merge_temp_bytes("u32", k, n)
+        temp = torch.empty(max(temp_bytes, 1), dtype=torch.uint8, device="cuda")
+        stream = torch.cuda.Stream()
+        times = []
+        for i in range(reps + 1):
+            ctx.set_profiling(i > 0)
+            with torch.cuda.stream(stream):
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                ctx.kway_merge_device(ptrs, lens, out.data_ptr(), "u32", temp.data_ptr(), temp_bytes,
+                                      stream.cuda_stream)
+                b.record(stream)
+            stream.synchronize()
+            if i > 0:
+                times.append(a.elapsed_time(b))
+        kt = ctx.kernel_times()
+        ctx.set_profiling(False)
+        ok = verify_sorted_permutation(torch, out, src, "u32")
+        ms = statistics.median(times)
+        alg = 2 * 4 * n
+        line = {"sweep": "kway_merge", "dtype": "u32", "n": n, "k": k, "run_lengths": "Dirichlet(1)", "ms": ms,
+                "keys_per_s": n / (ms / 1e3), "hbm_alg_gbs": alg / (ms / 1e3) / 1e9,
+                "roofline_frac": alg / (ms / 1e3) / 1e9 / peak, "verified": ok,
+                "kernels": {k_: {"launches": v[0] // reps, "ms": v[1] / reps} for k_, v in kt.items()}}
+        # cpu_baseline: the reference's own CPU merge (__gnu_parallel::multiway_merge through oracle/_ref)
+        # on a bounded sample: the first 2^27 keys split into k runs of the same proportions.
+        if orc is None:
+            orc = load_oracle()
+        if orc.ref_available():
+            m = 1 << 27
+            sl = [max(1, int(x * m / n)) for x in lens]
+            host_runs = []
+            hsrc = src[: sum(sl)].cpu().numpy().view(np.uint32)
+            o = 0
+            for x in sl:
+                host_runs.append(np.sort(hsrc[o:o + x]))
+                o += x
+            threads = os.cpu_count() or 1
+            t0 = time.perf_counter()
+            orc.ref_multiway_merge(host_runs, threads)
+            dt = time.perf_counter() - t0
+            line["cpu_baseline"] = {"value": sum(sl) / dt, "unit": "keys/s", "cores": threads, "kind": "reference",
+                                    "sample": f"{sum(sl)} keys in {k} runs of the same proportions "
+                                              "(__gnu_parallel::multiway_merge, src/gowanlock_sort.cuh:73-74)"}
+        print(json.dumps(line), flush=True)
+        del runs, temp
+    ctx.close()
+
+
+def link_bandwidth(torch, nbytes=1 << 32):
+    """Pinned host<->device copy bandwidth (GB/s): H2D alone, D2H alone, and both at once (full duplex)."""
+    h_in = torch.empty(nbytes, dtype=torch.uint8).pin_memory()
+    h_out = torch.empty(nbytes, dtype=torch.uint8).pin_memory()
+    d_a = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    d_b = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    s1, s2 = torch.cuda.Stream(), torch.cuda.Stream()
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        fn()
+        torch.cuda.synchronize()
+        return time.perf_counter() - t0
+
+    def h2d():
+        with torch.cuda.stream(s1):
+            d_a.copy_(h_in, non_blocking=True)
+
+    def d2h():
+        with torch.cuda.stream(s2):
+            h_out.copy_(d_b, non_blocking=True)
+
+    def both():
+        h2d()
+        d2h()
+
+    h2d(), d2h()
+    t_h2d, t_d2h, t_both = timed(h2d), timed(d2h), timed(both)
+    return {"h2d_gbs": nbytes / t_h2d / 1e9, "d2h_gbs": nbytes / t_d2h / 1e9,
+            "duplex_gbs_each": nbytes / t_both / 1e9, "bytes": nbytes}
+
+
+def sweep_ooc(mgs, torch, n, chunk=1 << 28):
+    """Out-of-core GowanlockSort pipeline over n uint64 keys in pinned host memory, chunks of `chunk` keys,
+    with the GPU k-way merge and with the reference's CPU multiway merge; end-to-end keys/s against the
+    host-link bound (every key crosses the link twice per direction with the GPU merge, once with the CPU
+    merge)."""
+    link = link_bandwidth(torch)
+    print(json.dumps({"sweep": "link", **link}), flush=True)
+    ctx = mgs.Context(0)
+    h = mgs.host_empty(n, np.uint64)
+    for merge_on_gpu in (True, False):
+        mgs.generate("u64", "full-uniform", SEED, n, out=h)
+        x0 = int(np.bitwise_xor.reduce(h))
+        s0 = int(h.sum(dtype=np.uint64))
+        t0 = time.perf_counter()
+        ctx.gowanlock_sort(h, chunk_size=chunk, merge_group_size=0, num_buffers=3, merge_on_gpu=merge_on_gpu)
+        dt = time.perf_counter() - t0
+        phases = {p: ctx.phase_seconds(p) for p in ("memory_allocation", "sort_phase", "merge_phase")}
+        ok = True
+        step = 1 << 28
+        for o in range(0, n, step):
+            seg = h[o:min(n, o + step + 1)]
+            if not bool(np.all(seg[1:] >= seg[:-1])):
+                ok = False
+                break
+        ok = ok and int(np.bitwise_xor.reduce(h)) == x0 and int(h.sum(dtype=np.uint64)) == s0
+        w = 8
+        crossings = 2 if merge_on_gpu else 1
+        bound_s = crossings * n * w / (min(link["duplex_gbs_each"], link["h2d_gbs"], link["d2h_gbs"]) * 1e9)
+        print(json.dumps({"sweep": "out_of_core", "dtype": "u64", "n": n, "bytes": n * w, "chunk": chunk,
+                          "num_buffers": 3, "merge": "gpu" if merge_on_gpu else "cpu (reference multiway_merge)",
+                          "s": dt, "keys_per_s": n / dt, "phases_s": phases,
+                          "link_bound_s": bound_s, "link_frac": bound_s / dt, "verified": ok}), flush=True)
+    ctx.close()
+
+
 def cpu_reference_sort(orc, base: np.ndarray, budget_s: float, max_reps: int):
     """Times the reference's gnu_parallel sort on copies of `base` (bounded)."""
     threads = orc.ref_num_procs()
@@ -320,6 +585,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched (segmented) measurement")
     ap.add_argument("--no-served", action="store_true", help="skip the serving-loop measurement")
+    ap.add_argument("--sweep", choices=["types", "merge", "ooc"],
+                    help="measure another workload of the sort API instead (one JSON line per case)")
+    ap.add_argument("--sweep-n", type=int, default=0, help="keys per case of --sweep (0: the workload's default)")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -328,6 +596,18 @@ def main():
 
     if args.impl == "reference":
         run_reference(args, rank)
+        return
+
+    if args.sweep:
+        import torch
+        torch.cuda.set_device(local_rank)
+        mgs = load_mgs()
+        if args.sweep == "types":
+            sweep_types(mgs, torch, args.sweep_n or N_KEYS)
+        elif args.sweep == "merge":
+            sweep_merge(mgs, torch, args.sweep_n or (1 << 31))
+        else:
+            sweep_ooc(mgs, torch, args.sweep_n or (1 << 32))
         return
 
     import torch

@@ -218,17 +218,38 @@ __global__ __launch_bounds__(128) void kway_partition_kernel(
 }
 
 // ---------------------------------------------------------------- K5/K7b ----
+// One output tile (BLOCK * ITEMS keys) of a stable k-way merge. The tile's
+// slice of every run (from the split matrix) is staged back to back in run
+// order in shared memory; then ceil(log2 k) rounds merge neighbouring slices
+// pairwise. In a round every thread finds where its ITEMS consecutive outputs
+// start in their pair (merge-path search) and merges them serially into
+// registers, with one comparison, one select and one shared-memory load per
+// key; the last round stores its registers straight to global memory.
+// The shared buffers carry one pad element per 128 bytes (a thread's outputs
+// sit ITEMS positions from its neighbour's, which without the pad fall into a
+// few banks) and spare elements at the end (the serial merge may load one key
+// past its slice; that key is never used).
+template <typename Bits>
+__device__ __forceinline__ uint32_t tile_pad(uint32_t i) {
+  return i + i / uint32_t(128 / sizeof(Bits));
+}
+template <typename Bits>
+constexpr size_t tile_buffer_elems(size_t tile) {
+  return (tile + tile / (128 / sizeof(Bits)) + 1 + 3) / 4 * 4;
+}
+
 template <class Tr, int BLOCK, int ITEMS>
 __global__ __launch_bounds__(BLOCK) void tile_merge_kernel(const typename Tr::Bits* const* __restrict__ runs, int k,
                                                            const u64* __restrict__ splits,
                                                            typename Tr::Bits* __restrict__ out, u64 total, u64 tile0) {
   using Bits = typename Tr::Bits;
   constexpr int kTile = BLOCK * ITEMS;
+  constexpr uint32_t kBuf = uint32_t(tile_buffer_elems<Bits>(kTile));
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Bits* buf0 = reinterpret_cast<Bits*>(smem_raw);
-  Bits* buf1 = buf0 + kTile;
-  u64* sstart = reinterpret_cast<u64*>(buf1 + kTile);
-  uint32_t* seg0 = reinterpret_cast<uint32_t*>(sstart + k);
+  Bits* buf1 = buf0 + kBuf;
+  const Bits** sptr = reinterpret_cast<const Bits**>(buf1 + kBuf);  // this tile's first key of every run
+  uint32_t* seg0 = reinterpret_cast<uint32_t*>(sptr + k);
   uint32_t* seg1 = seg0 + (k + 1);
   __shared__ uint32_t scan_tmp[BLOCK / 32 + 1];
 
@@ -237,14 +258,14 @@ __global__ __launch_bounds__(BLOCK) void tile_merge_kernel(const typename Tr::Bi
   const u64 d0 = j * u64(kTile);
   const uint32_t cnt = uint32_t(min(u64(kTile), total - d0));
 
-  // Segment offsets of the k input ranges (exclusive scan of their lengths).
+  // Segment offsets of the k input slices (exclusive scan of their lengths).
   const int per_thread = (k + BLOCK - 1) / BLOCK;
   uint32_t local = 0;
   for (int i = 0; i < per_thread; ++i) {
     const int r = tid * per_thread + i;
     if (r < k) {
       const u64 s = splits[j * k + r];
-      sstart[r] = s;
+      sptr[r] = runs[r] + s;
       local += uint32_t(splits[(j + 1) * k + r] - s);
     }
   }
@@ -254,86 +275,142 @@ __global__ __launch_bounds__(BLOCK) void tile_merge_kernel(const typename Tr::Bi
     const int r = tid * per_thread + i;
     if (r < k) {
       seg0[r] = run_off;
-      run_off += uint32_t(splits[(j + 1) * k + r] - sstart[r]);
+      run_off += uint32_t(splits[(j + 1) * k + r] - splits[j * k + r]);
     }
   }
   if (tid == 0) seg0[k] = cnt;
   __syncthreads();
 
-  // Stage the k ranges back to back in run order.
-  for (uint32_t i = tid; i < cnt; i += BLOCK) {
-    int lo = 0, hi = k;  // largest r with seg0[r] <= i
-    while (hi - lo > 1) {
-      const int mid = (lo + hi) >> 1;
-      if (seg0[mid] <= i) {
-        lo = mid;
-      } else {
-        hi = mid;
-      }
-    }
-    buf0[i] = runs[lo][sstart[lo] + (i - seg0[lo])];
-  }
-  __syncthreads();
-
-  // Pairwise merge rounds in shared memory.
-  Bits* src = buf0;
-  Bits* dst = buf1;
-  uint32_t* so = seg0;
-  uint32_t* no = seg1;
-  int m = k;
-  while (m > 1) {
-    const int m2 = (m + 1) / 2;
-    for (int i = tid; i <= m2; i += BLOCK) no[i] = (i < m2) ? so[2 * i] : cnt;
-    __syncthreads();
-    uint32_t p = uint32_t(tid) * ITEMS;
-    const uint32_t p1 = min(p + ITEMS, cnt);
-    if (p < p1) {
-      int lo = 0, hi = m2;  // pair containing p: largest q with no[q] <= p
+  // Stage the slices back to back: consecutive threads read consecutive keys;
+  // every thread issues its ITEMS loads before storing any. A thread's
+  // elements are BLOCK apart, so its slice index only moves forward.
+  {
+    Bits v[ITEMS];
+    int r = 0;
+    {
+      int lo = 0, hi = k;  // largest r with seg0[r] <= tid
       while (hi - lo > 1) {
         const int mid = (lo + hi) >> 1;
-        if (no[mid] <= p) {
+        if (seg0[mid] <= uint32_t(tid)) {
           lo = mid;
         } else {
           hi = mid;
         }
       }
-      int q = lo;
-      while (p < p1) {
-        const uint32_t a0 = so[2 * q];
-        const uint32_t a1 = so[min(2 * q + 1, m)];
-        const uint32_t b1 = so[min(2 * q + 2, m)];
-        const Bits* A = src + a0;
-        const Bits* B = src + a1;
-        const uint32_t la = a1 - a0, lb = b1 - a1;
-        const uint32_t diag = p - a0;
-        uint32_t s_lo = diag > lb ? diag - lb : 0, s_hi = min(diag, la);
-        while (s_lo < s_hi) {
-          const uint32_t mid = (s_lo + s_hi) >> 1;
-          if (!Tr::Less(B[diag - 1 - mid], A[mid])) {
-            s_lo = mid + 1;
-          } else {
-            s_hi = mid;
-          }
+      r = lo;
+    }
+    // The current slice in registers: its end and the address of tile
+    // position 0 in its run (slice start minus the slice's tile offset).
+    uint32_t r_end = seg0[r + 1];
+    const Bits* r_base = sptr[r] - seg0[r];
+#pragma unroll
+    for (int t = 0; t < ITEMS; ++t) {
+      const uint32_t i = uint32_t(t) * BLOCK + tid;
+      if (i < cnt) {
+        if (i >= r_end) {
+          do {
+            ++r;
+          } while (seg0[r + 1] <= i);  // seg0[k] = cnt > i ends the walk
+          r_end = seg0[r + 1];
+          r_base = sptr[r] - seg0[r];
         }
-        uint32_t ia = s_lo, ib = diag - s_lo;
-        Bits va = ia < la ? A[ia] : Bits(0);
-        Bits vb = ib < lb ? B[ib] : Bits(0);
-        const uint32_t pend = min(p1, b1);
-        while (p < pend) {
-          const bool take_b = ib < lb && (ia >= la || Tr::Less(vb, va));
-          if (take_b) {
-            dst[p++] = vb;
-            ++ib;
-            if (ib < lb) vb = B[ib];
-          } else {
-            dst[p++] = va;
-            ++ia;
-            if (ia < la) va = A[ia];
-          }
-        }
-        ++q;
+        v[t] = __ldg(r_base + i);
       }
     }
+#pragma unroll
+    for (int t = 0; t < ITEMS; ++t) {
+      const uint32_t i = uint32_t(t) * BLOCK + tid;
+      if (i < cnt) buf0[tile_pad<Bits>(i)] = v[t];
+    }
+  }
+  __syncthreads();
+
+  // Pairwise merge rounds.
+  Bits* src = buf0;
+  Bits* dst = buf1;
+  uint32_t* so = seg0;
+  uint32_t* no = seg1;
+  int m = k;
+  const uint32_t p0 = uint32_t(tid) * ITEMS;
+  const uint32_t nv = p0 < cnt ? min(uint32_t(ITEMS), cnt - p0) : 0u;  // outputs of this thread
+  for (;;) {
+    const int m2 = (m + 1) / 2;
+    for (int i = tid; i <= m2; i += BLOCK) no[i] = (i < m2) ? so[2 * i] : cnt;
+    __syncthreads();
+    Bits v[ITEMS];
+    if (nv > 0) {
+      int q = 0, hi = m2;  // pair holding p0: largest q with no[q] <= p0
+      while (hi - q > 1) {
+        const int mid = (q + hi) >> 1;
+        if (no[mid] <= p0) {
+          q = mid;
+        } else {
+          hi = mid;
+        }
+      }
+      // Pair q: A = [a0, a1), B = [a1, b1) (B empty for the odd slice out).
+      uint32_t a0 = so[2 * q], a1 = so[min(2 * q + 1, m)], b1 = so[min(2 * q + 2, m)];
+      const uint32_t la = a1 - a0, lb = b1 - a1;
+      const uint32_t diag = p0 - a0;
+      uint32_t s_lo = diag > lb ? diag - lb : 0, s_hi = min(diag, la);
+      while (s_lo < s_hi) {
+        const uint32_t mid = (s_lo + s_hi) >> 1;
+        if (!Tr::Less(src[tile_pad<Bits>(a1 + diag - 1 - mid)], src[tile_pad<Bits>(a0 + mid)])) {
+          s_lo = mid + 1;
+        } else {
+          s_hi = mid;
+        }
+      }
+      uint32_t ia = a0 + s_lo, ib = a1 + (diag - s_lo), a_end = a1, b_end = b1;
+      Bits ka = src[tile_pad<Bits>(ia)];
+      Bits kb = src[tile_pad<Bits>(ib)];
+#pragma unroll
+      for (int i = 0; i < ITEMS; ++i) {
+        if (uint32_t(i) < nv) {
+          while (p0 + i == b_end) {  // this thread's outputs continue in the next non-empty pair
+            ++q;
+            ia = b_end;
+            a_end = so[min(2 * q + 1, m)];
+            ib = a_end;
+            b_end = so[min(2 * q + 2, m)];
+            ka = src[tile_pad<Bits>(ia)];
+            kb = src[tile_pad<Bits>(ib)];
+          }
+          const bool take_a = ia < a_end && (ib >= b_end || !Tr::Less(kb, ka));
+          v[i] = take_a ? ka : kb;
+          ia += take_a ? 1u : 0u;
+          ib += take_a ? 0u : 1u;
+          const Bits kn = src[tile_pad<Bits>(take_a ? ia : ib)];
+          ka = take_a ? kn : ka;
+          kb = take_a ? kb : kn;
+        }
+      }
+    }
+    if (m2 == 1) {
+      Bits* o = out + d0 + p0;
+      if (nv == uint32_t(ITEMS) && (reinterpret_cast<uintptr_t>(o) & 15u) == 0) {
+        constexpr int kPerVec = 16 / int(sizeof(Bits));
+#pragma unroll
+        for (int i = 0; i < ITEMS; i += kPerVec) {
+          uint4 q4;
+          if constexpr (sizeof(Bits) == 4) {
+            q4 = make_uint4(uint32_t(v[i]), uint32_t(v[i + 1]), uint32_t(v[i + 2]), uint32_t(v[i + 3]));
+          } else {
+            q4 = make_uint4(uint32_t(v[i]), uint32_t(uint64_t(v[i]) >> 32), uint32_t(v[i + 1]),
+                            uint32_t(uint64_t(v[i + 1]) >> 32));
+          }
+          *reinterpret_cast<uint4*>(o + i) = q4;
+        }
+      } else {
+#pragma unroll
+        for (int i = 0; i < ITEMS; ++i)
+          if (uint32_t(i) < nv) o[i] = v[i];
+      }
+      return;
+    }
+#pragma unroll
+    for (int i = 0; i < ITEMS; ++i)
+      if (uint32_t(i) < nv) dst[tile_pad<Bits>(p0 + i)] = v[i];
     __syncthreads();
     Bits* t = src;
     src = dst;
@@ -343,8 +420,6 @@ __global__ __launch_bounds__(BLOCK) void tile_merge_kernel(const typename Tr::Bi
     no = ts;
     m = m2;
   }
-
-  for (uint32_t i = tid; i < cnt; i += BLOCK) out[d0 + i] = src[i];
 }
 
 // ---------------------------------------------------------------- host ------
@@ -468,9 +543,10 @@ cudaError_t kway_merge_typed(const void* const* runs_v, const size_t* lens, int 
   }
   if (e != cudaSuccess) return e;
   auto kernel = tile_merge_kernel<Tr, Shape::kBlock, Shape::kItems>;
-  const size_t smem = 2 * kTile * sizeof(Bits) + size_t(k) * 8 + size_t(2 * (k + 1)) * 4;
+  const size_t bufs = 2 * tile_buffer_elems<Bits>(kTile) * sizeof(Bits);
+  const size_t smem = bufs + size_t(k) * 8 + size_t(2 * (k + 1)) * 4;
   static SmemLimitOnce attr;
-  e = attr.ensure(kernel, 2 * kTile * sizeof(Bits) + size_t(kMaxKwayRuns) * 8 + size_t(2 * (kMaxKwayRuns + 1)) * 4);
+  e = attr.ensure(kernel, bufs + size_t(kMaxKwayRuns) * 8 + size_t(2 * (kMaxKwayRuns + 1)) * 4);
   if (e != cudaSuccess) return e;
   // Output tiles in windows of about window_keys keys (one window when 0).
   const u64 per_window =
