@@ -115,7 +115,9 @@ constexpr int kMaxRunsPerLane = kMaxKwayRuns / 32;
 // One warp per diagonal d: splits[r] = number of elements of run r among the
 // first d outputs of the stable k-way merge. Optional coarse level: the
 // splits / ub / lt / v* of the enclosing coarse diagonals bound the search.
-template <class Tr>
+// Lane l handles runs l, l + 32, ... (PER_LANE of them, PER_LANE >= k / 32),
+// with its per-run search windows in registers.
+template <class Tr, int PER_LANE>
 __global__ __launch_bounds__(128) void kway_partition_kernel(
     const typename Tr::Bits* const* __restrict__ runs, const u64* __restrict__ lens, int k, u64 total, u64 spacing,
     u64 num_diag, const u64* __restrict__ c_splits, const u64* __restrict__ c_ub, const u64* __restrict__ c_lt,
@@ -126,9 +128,9 @@ __global__ __launch_bounds__(128) void kway_partition_kernel(
   const int lane = threadIdx.x & 31;
   if (w >= num_diag) return;
   const u64 d = min(w * spacing, total);
-  const int per_lane = (k + 31) / 32;
   if (d >= total) {
-    for (int i = 0; i < per_lane; ++i) {
+#pragma unroll
+    for (int i = 0; i < PER_LANE; ++i) {
       const int r = lane + 32 * i;
       if (r < k) {
         splits[w * k + r] = lens[r];
@@ -139,7 +141,7 @@ __global__ __launch_bounds__(128) void kway_partition_kernel(
     if (vstar_out && lane == 0) vstar_out[w] = ~Bits(0);
     return;
   }
-  u64 a[kMaxRunsPerLane], b[kMaxRunsPerLane], base[kMaxRunsPerLane];
+  u64 a[PER_LANE], b[PER_LANE], base[PER_LANE];
   Bits vlo = 0, vhi = ~Bits(0);
   u64 c0 = 0, c1 = 0;
   if (c_splits) {
@@ -148,7 +150,8 @@ __global__ __launch_bounds__(128) void kway_partition_kernel(
     vlo = c_vstar[c0];
     vhi = c_vstar[c1];
   }
-  for (int i = 0; i < per_lane; ++i) {
+#pragma unroll
+  for (int i = 0; i < PER_LANE; ++i) {
     const int r = lane + 32 * i;
     if (r < k) {
       a[i] = c_splits ? c_splits[c0 * k + r] : 0;
@@ -161,12 +164,14 @@ __global__ __launch_bounds__(128) void kway_partition_kernel(
   // Bisection for v* = the smallest v with (number of keys <= v) > d.
   while (vlo < vhi) {
     u64 width = 0;
-    for (int i = 0; i < per_lane; ++i) width += b[i] - a[i];
+#pragma unroll
+    for (int i = 0; i < PER_LANE; ++i) width += b[i] - a[i];
     if (warp_sum_u64<Bits>(width) == 0) break;  // no key strictly inside: v* = vlo
     const Bits vmid = vlo + (vhi - vlo) / 2;
-    u64 u[kMaxRunsPerLane];
+    u64 u[PER_LANE];
     u64 cnt = 0;
-    for (int i = 0; i < per_lane; ++i) {
+#pragma unroll
+    for (int i = 0; i < PER_LANE; ++i) {
       const int r = lane + 32 * i;
       u[i] = (r < k) ? bound_search<Tr, true>(runs[r], a[i], b[i], vmid) : 0;
       cnt += u[i];
@@ -174,17 +179,20 @@ __global__ __launch_bounds__(128) void kway_partition_kernel(
     const u64 le = warp_sum_u64<Bits>(cnt);
     if (le > d) {
       vhi = vmid;
-      for (int i = 0; i < per_lane; ++i) b[i] = u[i];
+#pragma unroll
+      for (int i = 0; i < PER_LANE; ++i) b[i] = u[i];
     } else {
       vlo = vmid + 1;
-      for (int i = 0; i < per_lane; ++i) a[i] = base[i] = u[i];
+#pragma unroll
+      for (int i = 0; i < PER_LANE; ++i) a[i] = base[i] = u[i];
     }
   }
   const Bits vs = vlo;
   // Keys equal to v* are split across runs in run order (stability).
-  u64 lt[kMaxRunsPerLane], eq[kMaxRunsPerLane];
+  u64 lt[PER_LANE], eq[PER_LANE];
   u64 lt_sum = 0;
-  for (int i = 0; i < per_lane; ++i) {
+#pragma unroll
+  for (int i = 0; i < PER_LANE; ++i) {
     const int r = lane + 32 * i;
     if (r < k) {
       lt[i] = bound_search<Tr, false>(runs[r], base[i], b[i], vs);
@@ -199,7 +207,8 @@ __global__ __launch_bounds__(128) void kway_partition_kernel(
   }
   const u64 rem = d - warp_sum_u64<Bits>(lt_sum);
   u64 before = 0;  // equal keys in all runs with a lower index
-  for (int i = 0; i < per_lane; ++i) {
+#pragma unroll
+  for (int i = 0; i < PER_LANE; ++i) {
     u64 incl = eq[i];
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -474,6 +483,20 @@ KwayLayout kway_layout(int k, size_t total) {
   return L;
 }
 
+// kway_partition_kernel with the smallest runs-per-lane count that covers k.
+template <class Tr, typename... Args>
+cudaError_t launch_partition(LaunchRecorder* rec, int k, dim3 grid, cudaStream_t stream, Args... args) {
+  const int per_lane = (k + 31) / 32;
+#define MGS_PARTITION(L) \
+  launch_kernel(rec, "kway_partition", kway_partition_kernel<Tr, L>, grid, dim3(128), 0, stream, args...)
+  if (per_lane <= 1) return MGS_PARTITION(1);
+  if (per_lane <= 2) return MGS_PARTITION(2);
+  if (per_lane <= 4) return MGS_PARTITION(4);
+  if (per_lane <= 8) return MGS_PARTITION(8);
+  return MGS_PARTITION(kMaxRunsPerLane);
+#undef MGS_PARTITION
+}
+
 template <class Tr>
 cudaError_t kway_merge_typed(const void* const* runs_v, const size_t* lens, int k, void* out_v, void* temp,
                              size_t temp_bytes, size_t window_keys, const MergeWindowFn& on_window,
@@ -526,20 +549,19 @@ cudaError_t kway_merge_typed(const void* const* runs_v, const size_t* lens, int 
       u64* cl = reinterpret_cast<u64*>(tb + L.c_lt_off);
       Bits* cv = reinterpret_cast<Bits*>(tb + L.c_vstar_off);
       const u64 cdiag = L.num_coarse + 1;
-      e = launch_kernel(rec, "kway_partition", kway_partition_kernel<Tr>, dim3(unsigned((cdiag * 32 + 127) / 128)),
-                        dim3(128), 0, stream, d_runs, d_lens, k, u64(total), c_spacing, cdiag,
-                        static_cast<const u64*>(nullptr), static_cast<const u64*>(nullptr),
-                        static_cast<const u64*>(nullptr), static_cast<const Bits*>(nullptr), u64(1), cs, cu, cl, cv);
+      e = launch_partition<Tr>(rec, k, dim3(unsigned((cdiag * 32 + 127) / 128)), stream, d_runs, d_lens, k,
+                               u64(total), c_spacing, cdiag, static_cast<const u64*>(nullptr),
+                               static_cast<const u64*>(nullptr), static_cast<const u64*>(nullptr),
+                               static_cast<const Bits*>(nullptr), u64(1), cs, cu, cl, cv);
       if (e != cudaSuccess) return e;
       c_splits = cs;
       c_ub = cu;
       c_lt = cl;
       c_vstar = cv;
     }
-    e = launch_kernel(rec, "kway_partition", kway_partition_kernel<Tr>, dim3(unsigned((num_diag * 32 + 127) / 128)),
-                      dim3(128), 0, stream, d_runs, d_lens, k, u64(total), kTile, num_diag, c_splits, c_ub, c_lt,
-                      c_vstar, c_spacing, d_splits, static_cast<u64*>(nullptr), static_cast<u64*>(nullptr),
-                      static_cast<Bits*>(nullptr));
+    e = launch_partition<Tr>(rec, k, dim3(unsigned((num_diag * 32 + 127) / 128)), stream, d_runs, d_lens, k,
+                             u64(total), kTile, num_diag, c_splits, c_ub, c_lt, c_vstar, c_spacing, d_splits,
+                             static_cast<u64*>(nullptr), static_cast<u64*>(nullptr), static_cast<Bits*>(nullptr));
   }
   if (e != cudaSuccess) return e;
   auto kernel = tile_merge_kernel<Tr, Shape::kBlock, Shape::kItems>;
