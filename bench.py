@@ -164,6 +164,13 @@ def batched_bench(mgs, torch, ctx):
             times.append(ev[0].elapsed_time(ev[1]))
     ctx.synchronize()
     batched_ms = statistics.median(times)
+    direct_result = work.clone()
+    # the same launches recorded once into a CUDA graph (mgs_plan_segmented_create) and replayed
+    graph_ms, graph_same = replay_ms(ctx, torch, stream, work, pristine, direct_result,
+                                     lambda: ctx.plan_segmented(work.data_ptr(), n, d_offs.data_ptr(), offs.size - 1,
+                                                                "u32", temp.data_ptr(), temp_bytes), reps=3)
+    del direct_result
+    small = small_batch_bench(mgs, torch, ctx, stream)
     # plain form: one sort launch sequence per segment, same stream
     plain_temp = mgs.Context.sort_temp_bytes("u32", int(np.diff(offs).max()))
     ptemp = torch.empty(plain_temp, dtype=torch.uint8, device="cuda")
@@ -186,7 +193,64 @@ def batched_bench(mgs, torch, ctx):
             "segments_le_256": int((lens <= 256).sum()), "segments_gt_16384": int((lens > 16384).sum()),
             "batched_ms": batched_ms, "batched_keys_per_s": n / (batched_ms / 1e3),
             "plain_ms": plain_ms, "plain_keys_per_s": n / (plain_ms / 1e3),
-            "speedup_vs_plain": plain_ms / batched_ms}
+            "speedup_vs_plain": plain_ms / batched_ms,
+            "graph_ms": graph_ms, "graph_same_result": graph_same, "small_batch": small}
+
+
+def replay_ms(ctx, torch, stream, work, pristine, expected, make_plan, reps):
+    """Median CUDA-event time of `reps` replays of a recorded plan (input restored before each, outside the
+    timed region) and whether the last replay's result equals `expected`."""
+    plan = make_plan()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    times = []
+    try:
+        for i in range(reps + 1):
+            with torch.cuda.stream(stream):
+                work.copy_(pristine)
+                ev[0].record(stream)
+                plan.launch(stream.cuda_stream)
+                ev[1].record(stream)
+            stream.synchronize()
+            if i > 0:
+                times.append(ev[0].elapsed_time(ev[1]))
+        ctx.synchronize()
+        same = bool(torch.equal(work, expected))
+    finally:
+        plan.close()
+    return statistics.median(times), same
+
+
+def small_batch_bench(mgs, torch, ctx, stream, reps=20):
+    """A small batch (1024 Zipf(1.2) segments, 2^18 u32 keys) where launch overhead matters: the direct
+    segmented call against its recorded CUDA graph, median CUDA-event time per call."""
+    rng = np.random.default_rng(12)
+    offs = zipf_segment_offsets(rng, nseg=1024, total=1 << 18, max_len=1 << 14)
+    n = int(offs[-1])
+    pristine = torch.from_numpy(mgs.generate("u32", "full-uniform", 6, n).view(np.int32)).cuda()
+    work = torch.empty_like(pristine)
+    d_offs = torch.from_numpy(offs).cuda()
+    temp_bytes = mgs.Context.segmented_sort_temp_bytes("u32", n, offs.size - 1)
+    temp = torch.empty(temp_bytes, dtype=torch.uint8, device="cuda")
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    times = []
+    for i in range(reps + 1):
+        with torch.cuda.stream(stream):
+            work.copy_(pristine)
+            ev[0].record(stream)
+            ctx.segmented_sort_device(work.data_ptr(), n, d_offs.data_ptr(), offs.size - 1, "u32", temp.data_ptr(),
+                                      temp_bytes, stream.cuda_stream)
+            ev[1].record(stream)
+        stream.synchronize()
+        if i > 0:
+            times.append(ev[0].elapsed_time(ev[1]))
+    ctx.synchronize()
+    direct_ms = statistics.median(times)
+    expected = work.clone()
+    graph_ms, same = replay_ms(ctx, torch, stream, work, pristine, expected,
+                               lambda: ctx.plan_segmented(work.data_ptr(), n, d_offs.data_ptr(), offs.size - 1, "u32",
+                                                          temp.data_ptr(), temp_bytes), reps)
+    return {"segments": int(offs.size - 1), "keys": n, "direct_ms": direct_ms, "graph_ms": graph_ms,
+            "graph_same_result": same}
 
 
 def served_bench(mgs, budget_s=2.0):

@@ -175,6 +175,28 @@ int mgs_segmented_sort_temp_bytes(int dtype, size_t n, size_t num_segments, size
 int mgs_segmented_sort_device(mgs_ctx* ctx, int dtype, void* d_keys, size_t n, const uint64_t* d_offsets,
                               size_t num_segments, void* d_temp, size_t temp_bytes, void* stream);
 
+/* ---- recorded sorts (CUDA graphs) -------------------------------------------
+ * No counterpart in the reference (its sorts are host-driven thrust calls). A
+ * plan records once, into a CUDA graph, the launches of one device sort or one
+ * segmented sort of a FIXED buffer (keys, offsets and scratch pointers are baked
+ * in); mgs_plan_launch replays them with a single graph launch on any stream,
+ * sorting whatever the buffer holds at that time. For callers that sort the same
+ * buffers again and again (a batch loop, a serving slot): one launch instead of
+ * seven or more, no host work per sort. d_temp NULL: the plan allocates and owns
+ * its scratch (mgs_sort_temp_bytes / mgs_segmented_sort_temp_bytes); otherwise
+ * the caller's scratch must outlive the plan. Device status goes to the
+ * context's status word (read by mgs_ctx_synchronize), so the context must
+ * outlive the plan. Creating a plan runs nothing on the GPU. Replays of one
+ * plan, or of two plans sharing scratch, must not overlap on the GPU. */
+typedef struct mgs_plan mgs_plan;
+int mgs_plan_sort_create(mgs_ctx* ctx, int dtype, void* d_keys, size_t n, void* d_temp, size_t temp_bytes,
+                         mgs_plan** out);
+int mgs_plan_segmented_create(mgs_ctx* ctx, int dtype, void* d_keys, size_t n, const uint64_t* d_offsets,
+                              size_t num_segments, void* d_temp, size_t temp_bytes, mgs_plan** out);
+int mgs_plan_launch(mgs_plan* plan, void* stream); /* NULL stream: the context's compute stream; asynchronous */
+int mgs_plan_launch_count(mgs_plan* plan, uint64_t* launches); /* kernel launches one replay performs */
+int mgs_plan_destroy(mgs_plan* plan); /* waits for the device first (replays may still run) */
+
 /* ---- GowanlockSort on one GPU: out-of-core chunk pipeline -------------------
  * (HET sort, src/gowanlock_sort.cuh:127-483). h_keys (host, pinned for full link
  * speed) is sorted in place. Phase 1 streams chunks of chunk_size keys through

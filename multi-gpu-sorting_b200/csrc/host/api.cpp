@@ -69,6 +69,87 @@ inline size_t align256(size_t x) { return (x + 255) / 256 * 256; }
 
 }  // namespace
 
+// A recorded sort: the instantiated CUDA graph of one sort's launches.
+struct mgs_plan {
+  mgs_ctx* ctx = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  void* owned_temp = nullptr;  // scratch the plan allocated itself
+  uint64_t launches = 0;       // kernel launches one replay performs
+};
+
+namespace {
+
+// Counts the launches issued while a plan is recorded (no timing events, which
+// would become graph nodes).
+struct CountingRecorder : mgs::LaunchRecorder {
+  uint64_t launches = 0;
+  void before(const char*, cudaStream_t) override { ++launches; }
+  void after(const char*, cudaStream_t) override {}
+};
+
+void plan_release(mgs_plan* p) {
+  if (!p) return;
+  if (p->exec) cudaGraphExecDestroy(p->exec);
+  if (p->graph) cudaGraphDestroy(p->graph);
+  if (p->owned_temp) cudaFree(p->owned_temp);
+  delete p;
+}
+
+// Records body(d_temp, temp_bytes, stream, recorder) into a graph on a private
+// stream (relaxed capture mode: the one-time per-kernel attribute calls the
+// launch path makes are allowed during the capture) and instantiates it.
+template <class Body>
+int plan_record(mgs_ctx* ctx, const char* what, size_t need, void* d_temp, size_t temp_bytes, Body body,
+                mgs_plan** out) {
+  Context& c = ctx->impl;
+  DeviceGuard g(c.device);
+  mgs_plan* p = new (std::nothrow) mgs_plan;
+  if (!p) {
+    set_last_error("%s: out of host memory", what);
+    return MGS_ERR_OOM;
+  }
+  p->ctx = ctx;
+  if (d_temp == nullptr) {
+    if (need > 0) {
+      const cudaError_t e = cudaMalloc(&p->owned_temp, need);
+      if (e != cudaSuccess) {
+        plan_release(p);
+        return cuda_fail(e, what);
+      }
+    }
+    d_temp = p->owned_temp;
+    temp_bytes = need;
+  } else if (temp_bytes < need) {
+    plan_release(p);
+    set_last_error("%s: d_temp holds %zu bytes, %zu needed", what, temp_bytes, need);
+    return MGS_ERR_INVALID;
+  }
+  cudaStream_t s = nullptr;
+  cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed);
+  if (e == cudaSuccess) {
+    CountingRecorder rec;
+    const cudaError_t eb = body(d_temp, temp_bytes, s, &rec);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ee = cudaStreamEndCapture(s, &graph);
+    p->graph = graph;
+    p->launches = rec.launches;
+    e = (eb != cudaSuccess) ? eb : ee;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&p->exec, p->graph, 0);
+  }
+  if (s) cudaStreamDestroy(s);
+  if (e != cudaSuccess) {
+    plan_release(p);
+    return cuda_fail(e, what);
+  }
+  *out = p;
+  mgs::clear_last_error();
+  return MGS_OK;
+}
+
+}  // namespace
+
 extern "C" {
 
 int mgs_version(void) { return 10000 * 0 + 100 * 1 + 0; }
@@ -457,6 +538,71 @@ int mgs_segmented_sort_device(mgs_ctx* ctx, int dtype, void* d_keys, size_t n, c
   cudaError_t e = mgs::segmented_sort(dtype, d_keys, n, d_offsets, num_segments, d_temp, temp_bytes, s, c.d_status,
                                       &c.recorder);
   if (e != cudaSuccess) return cuda_fail(e, "mgs_segmented_sort_device");
+  mgs::clear_last_error();
+  return MGS_OK;
+}
+
+int mgs_plan_sort_create(mgs_ctx* ctx, int dtype, void* d_keys, size_t n, void* d_temp, size_t temp_bytes,
+                         mgs_plan** out) {
+  if (!ctx || !out) return invalid("mgs_plan_sort_create: null argument");
+  *out = nullptr;
+  const size_t w = mgs::dtype_bytes(dtype);
+  if (w == 0) return invalid("mgs_plan_sort_create: unknown dtype");
+  if (n > 0 && !d_keys) return invalid("mgs_plan_sort_create: d_keys is null");
+  if (reinterpret_cast<uintptr_t>(d_keys) % w != 0) return invalid("mgs_plan_sort_create: d_keys is not key-aligned");
+  if (n > kMaxDeviceSortKeys) return invalid("mgs_plan_sort_create: n must be below 2^32");
+  const size_t need = n ? mgs::radix_sort_temp_bytes(dtype, n) : 0;
+  return plan_record(ctx, "mgs_plan_sort_create", need, d_temp, temp_bytes,
+                     [&](void* t, size_t tb, cudaStream_t s, mgs::LaunchRecorder* rec) {
+                       return mgs::radix_sort(dtype, d_keys, n, t, tb, s, ctx->impl.d_status, rec);
+                     },
+                     out);
+}
+
+int mgs_plan_segmented_create(mgs_ctx* ctx, int dtype, void* d_keys, size_t n, const uint64_t* d_offsets,
+                              size_t num_segments, void* d_temp, size_t temp_bytes, mgs_plan** out) {
+  if (!ctx || !out) return invalid("mgs_plan_segmented_create: null argument");
+  *out = nullptr;
+  const size_t w = mgs::dtype_bytes(dtype);
+  if (w == 0) return invalid("mgs_plan_segmented_create: unknown dtype");
+  const bool empty = (n == 0 || num_segments == 0);
+  if (!empty && (!d_keys || !d_offsets)) return invalid("mgs_plan_segmented_create: null pointer");
+  if (reinterpret_cast<uintptr_t>(d_keys) % w != 0)
+    return invalid("mgs_plan_segmented_create: d_keys is not key-aligned");
+  if (n > kMaxDeviceSortKeys || num_segments >= kMaxDeviceSortKeys)
+    return invalid("mgs_plan_segmented_create: n and num_segments must be below 2^32");
+  const size_t need = empty ? 0 : mgs::segmented_sort_temp_bytes(dtype, n, num_segments);
+  return plan_record(ctx, "mgs_plan_segmented_create", need, d_temp, temp_bytes,
+                     [&](void* t, size_t tb, cudaStream_t s, mgs::LaunchRecorder* rec) {
+                       if (empty) return cudaSuccess;
+                       return mgs::segmented_sort(dtype, d_keys, n, d_offsets, num_segments, t, tb, s,
+                                                  ctx->impl.d_status, rec);
+                     },
+                     out);
+}
+
+int mgs_plan_launch(mgs_plan* plan, void* stream) {
+  if (!plan) return invalid("mgs_plan_launch: plan is null");
+  Context& c = plan->ctx->impl;
+  DeviceGuard g(c.device);
+  const cudaError_t e = cudaGraphLaunch(plan->exec, stream ? static_cast<cudaStream_t>(stream) : c.compute);
+  if (e != cudaSuccess) return cuda_fail(e, "mgs_plan_launch");
+  c.recorder.add_launches(plan->launches);
+  mgs::clear_last_error();
+  return MGS_OK;
+}
+
+int mgs_plan_launch_count(mgs_plan* plan, uint64_t* launches) {
+  if (!plan || !launches) return invalid("mgs_plan_launch_count: null argument");
+  *launches = plan->launches;
+  return MGS_OK;
+}
+
+int mgs_plan_destroy(mgs_plan* plan) {
+  if (!plan) return MGS_OK;
+  DeviceGuard g(plan->ctx->impl.device);
+  cudaDeviceSynchronize();  // a replay may still run on any stream: let it finish before its graph and scratch go
+  plan_release(plan);
   mgs::clear_last_error();
   return MGS_OK;
 }

@@ -29,6 +29,7 @@ class EventRecorder : public LaunchRecorder {
   bool enabled() const { return enabled_; }
   uint64_t launches() const { return launches_; }
   void reset_launches() { launches_ = 0; }
+  void add_launches(uint64_t n) { launches_ += n; }  // launches replayed from a recorded plan
   // Synchronizes on the recorded events and folds them into per-name totals.
   cudaError_t collect(std::vector<std::pair<std::string, std::pair<uint64_t, double>>>* out);
 

@@ -116,6 +116,12 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "mgs_server_stats_get": ([c_void, ctypes.POINTER(ServerStats), c_int], c_int),
         "mgs_gowanlock_sort": ([c_void, c_int, c_void, c_size, c_size, c_size, c_size, c_int], c_int),
         "mgs_ctx_phase_seconds": ([c_void, ctypes.c_char_p, ctypes.POINTER(ctypes.c_double)], c_int),
+        "mgs_plan_sort_create": ([c_void, c_int, c_void, c_size, c_void, c_size, ctypes.POINTER(c_void)], c_int),
+        "mgs_plan_segmented_create": ([c_void, c_int, c_void, c_size, c_void, c_size, c_void, c_size,
+                                       ctypes.POINTER(c_void)], c_int),
+        "mgs_plan_launch": ([c_void, c_void], c_int),
+        "mgs_plan_launch_count": ([c_void, ctypes.POINTER(ctypes.c_uint64)], c_int),
+        "mgs_plan_destroy": ([c_void], c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -195,6 +201,37 @@ class DataGenerator:
 
     def compute_distribution(self, begin: np.ndarray, num_elements: int, distribution_type: str) -> None:
         generate(begin.dtype, distribution_type, self.distribution_seed, num_elements, out=begin)
+
+
+class Plan:
+    """A recorded sort (mgs_plan): launch() replays it on a stream; close() waits for the device and frees it.
+    The context that made it must stay open while the plan lives."""
+
+    def __init__(self, ctx: "Context", handle: ctypes.c_void_p):
+        self.ctx = ctx
+        self._lib = ctx._lib
+        self.handle = handle
+
+    def launch(self, stream: int = 0) -> None:
+        _check(self._lib.mgs_plan_launch(self.handle, ctypes.c_void_p(stream or None)))
+
+    def launch_count(self) -> int:
+        v = ctypes.c_uint64()
+        _check(self._lib.mgs_plan_launch_count(self.handle, ctypes.byref(v)))
+        return int(v.value)
+
+    def close(self) -> None:
+        """Frees the plan; a plan whose context was already closed is dropped without touching the context."""
+        if self.handle:
+            h, self.handle = self.handle, None
+            if self.ctx._fin.alive:
+                _check(self._lib.mgs_plan_destroy(h))
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Context:
@@ -295,6 +332,24 @@ class Context:
                                                    ctypes.c_void_p(d_offsets), int(num_segments),
                                                    ctypes.c_void_p(d_temp or None), int(temp_bytes),
                                                    ctypes.c_void_p(stream or None)))
+
+    # --- recorded sorts (CUDA graphs) ---
+    def plan_sort(self, d_keys: int, n: int, dtype, d_temp: int = 0, temp_bytes: int = 0) -> "Plan":
+        """Records the device sort of the fixed buffer d_keys[0..n) into a CUDA graph (mgs_plan_sort_create)."""
+        h = ctypes.c_void_p()
+        _check(self._lib.mgs_plan_sort_create(self.handle, dtype_code(dtype), ctypes.c_void_p(d_keys), int(n),
+                                              ctypes.c_void_p(d_temp or None), int(temp_bytes), ctypes.byref(h)))
+        return Plan(self, h)
+
+    def plan_segmented(self, d_keys: int, n: int, d_offsets: int, num_segments: int, dtype, d_temp: int = 0,
+                       temp_bytes: int = 0) -> "Plan":
+        """Records the segmented sort of fixed buffers into a CUDA graph (mgs_plan_segmented_create)."""
+        h = ctypes.c_void_p()
+        _check(self._lib.mgs_plan_segmented_create(self.handle, dtype_code(dtype), ctypes.c_void_p(d_keys), int(n),
+                                                   ctypes.c_void_p(d_offsets), int(num_segments),
+                                                   ctypes.c_void_p(d_temp or None), int(temp_bytes),
+                                                   ctypes.byref(h)))
+        return Plan(self, h)
 
     # --- GowanlockSort with one GPU: out-of-core chunk pipeline ---
     def gowanlock_sort(self, keys: np.ndarray, chunk_size: int = 0, merge_group_size: int = 0, num_buffers: int = 2,
