@@ -532,6 +532,18 @@ def sweep_merge(mgs, torch, n, reps=3):
     ctx.close()
 
 
+def sweep_tune(mgs, out_path, max_n=1 << 28, reps=3):
+    """Autotuner run: every onesweep variant (7 tile shapes x 2 ranking modes) timed per size class up to max_n
+    for 4- and 8-byte keys; the fastest per class goes into the table, which is written to out_path if given."""
+    ctx = mgs.Context(0)
+    for dtype in ("u32", "u64"):
+        for smp in ctx.autotune(dtype, max_n, reps):
+            print(json.dumps({"sweep": "tune", "dtype": dtype, **smp}), flush=True)
+    if out_path:
+        mgs.tune_save(out_path)
+    ctx.close()
+
+
 def link_bandwidth(torch, nbytes=1 << 32):
     """Pinned host<->device copy bandwidth (GB/s): H2D alone, D2H alone, and both at once (full duplex)."""
     h_in = torch.empty(nbytes, dtype=torch.uint8).pin_memory()
@@ -659,9 +671,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched (segmented) measurement")
     ap.add_argument("--no-served", action="store_true", help="skip the serving-loop measurement")
-    ap.add_argument("--sweep", choices=["types", "merge", "ooc"],
+    ap.add_argument("--sweep", choices=["types", "merge", "ooc", "tune"],
                     help="measure another workload of the sort API instead (one JSON line per case)")
     ap.add_argument("--sweep-n", type=int, default=0, help="keys per case of --sweep (0: the workload's default)")
+    ap.add_argument("--tune-out", default="", help="--sweep tune: write the tuned variant table to this file")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -678,6 +691,8 @@ def main():
         mgs = load_mgs()
         if args.sweep == "types":
             sweep_types(mgs, torch, args.sweep_n or N_KEYS)
+        elif args.sweep == "tune":
+            sweep_tune(mgs, args.tune_out, args.sweep_n or (1 << 28))
         elif args.sweep == "merge":
             sweep_merge(mgs, torch, args.sweep_n or (1 << 31))
         else:

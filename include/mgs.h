@@ -197,6 +197,36 @@ int mgs_plan_launch(mgs_plan* plan, void* stream); /* NULL stream: the context's
 int mgs_plan_launch_count(mgs_plan* plan, uint64_t* launches); /* kernel launches one replay performs */
 int mgs_plan_destroy(mgs_plan* plan); /* waits for the device first (replays may still run) */
 
+/* ---- onesweep variants and the autotuner ------------------------------------
+ * No counterpart in the reference (it calls thrust::sort with CUB's own tuning).
+ * The radix sort picks, per key width (4 or 8 bytes) and size class of n
+ * (0: n < 2^16, 1: < 2^18, 2: < 2^20, 3: < 2^22, 4: < 2^26, 5: larger), a tile
+ * shape (0..6: threads x keys per thread) and a ranking mode (2: shared-memory
+ * peer masks, 3: ballots for half of the keys). The table is read from a tuning
+ * file on first use (MGS_TUNE_FILE, else tuning/b200.tune beside the library's
+ * directory; format: lines "key_bytes size_class shape rank_mode"), and the
+ * environment variables MGS_ONESWEEP_SHAPE / MGS_RANK_MODE override it.
+ * mgs_autotune times every variant on a sample of each size class up to max_n
+ * (uniformly random keys of the dtype's width, median of reps sorts), keeps the
+ * fastest in the table and reports every timing in out (count = number of
+ * samples, also when more than capacity). It allocates and frees its own
+ * device buffers; no other sort may be issued meanwhile. Changing the table
+ * (set, load, autotune) while sorts are being issued from other threads races. */
+typedef struct mgs_tune_sample {
+  int key_bytes;
+  int size_class;
+  size_t n;
+  int shape;
+  int rank_mode;
+  double ms;
+  int chosen; /* 1 for the variant the table now holds for this class */
+} mgs_tune_sample;
+int mgs_tune_get(int dtype, size_t n, int* shape, int* rank_mode); /* the variant a sort of n keys uses */
+int mgs_tune_set(int dtype, int size_class, int shape, int rank_mode);
+int mgs_tune_load(const char* path);
+int mgs_tune_save(const char* path);
+int mgs_autotune(mgs_ctx* ctx, int dtype, size_t max_n, int reps, mgs_tune_sample* out, int capacity, int* count);
+
 /* ---- GowanlockSort on one GPU: out-of-core chunk pipeline -------------------
  * (HET sort, src/gowanlock_sort.cuh:127-483). h_keys (host, pinned for full link
  * speed) is sorted in place. Phase 1 streams chunks of chunk_size keys through

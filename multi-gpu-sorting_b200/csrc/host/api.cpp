@@ -9,6 +9,7 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <vector>
 
 #include "../kernels/engine_types.h"
 #include "../kernels/merge.cuh"
@@ -603,6 +604,71 @@ int mgs_plan_destroy(mgs_plan* plan) {
   DeviceGuard g(plan->ctx->impl.device);
   cudaDeviceSynchronize();  // a replay may still run on any stream: let it finish before its graph and scratch go
   plan_release(plan);
+  mgs::clear_last_error();
+  return MGS_OK;
+}
+
+int mgs_tune_get(int dtype, size_t n, int* shape, int* rank_mode) {
+  const size_t w = mgs::dtype_bytes(dtype);
+  if (w == 0 || !shape || !rank_mode) return invalid("mgs_tune_get: unknown dtype or null argument");
+  const mgs::SortVariant v = mgs::sort_variant(int(w), n);
+  *shape = v.shape;
+  *rank_mode = v.mode;
+  return MGS_OK;
+}
+
+int mgs_tune_set(int dtype, int size_class, int shape, int rank_mode) {
+  const size_t w = mgs::dtype_bytes(dtype);
+  if (w == 0) return invalid("mgs_tune_set: unknown dtype");
+  if (!mgs::set_sort_variant(int(w), size_class, mgs::SortVariant{shape, rank_mode})) {
+    set_last_error("mgs_tune_set: size_class must be in [0, %d), shape in [0, 7), rank_mode 2 or 3",
+                   mgs::kSizeClasses);
+    return MGS_ERR_INVALID;
+  }
+  mgs::clear_last_error();
+  return MGS_OK;
+}
+
+int mgs_tune_load(const char* path) {
+  if (!path) return invalid("mgs_tune_load: path is null");
+  const int r = mgs::load_tuning_file(path);
+  if (r == -1) {
+    set_last_error("mgs_tune_load: cannot open '%s'", path);
+    return MGS_ERR_INVALID;
+  }
+  if (r == -2) {
+    set_last_error("mgs_tune_load: '%s' has malformed or out-of-range lines (the valid ones were applied)", path);
+    return MGS_ERR_INVALID;
+  }
+  mgs::clear_last_error();
+  return MGS_OK;
+}
+
+int mgs_tune_save(const char* path) {
+  if (!path) return invalid("mgs_tune_save: path is null");
+  if (!mgs::save_tuning_file(path)) {
+    set_last_error("mgs_tune_save: cannot write '%s'", path);
+    return MGS_ERR_INVALID;
+  }
+  mgs::clear_last_error();
+  return MGS_OK;
+}
+
+int mgs_autotune(mgs_ctx* ctx, int dtype, size_t max_n, int reps, mgs_tune_sample* out, int capacity, int* count) {
+  if (!ctx) return invalid("mgs_autotune: ctx is null");
+  if (mgs::dtype_bytes(dtype) == 0) return invalid("mgs_autotune: unknown dtype");
+  if (reps < 1 || reps > 100) return invalid("mgs_autotune: reps must be in [1, 100]");
+  if (capacity > 0 && !out) return invalid("mgs_autotune: out is null");
+  Context& c = ctx->impl;
+  DeviceGuard g(c.device);
+  std::vector<mgs::TuneSample> samples;
+  const cudaError_t e = mgs::autotune(dtype, max_n, reps, &samples);
+  if (e != cudaSuccess) return cuda_fail(e, "mgs_autotune");
+  for (size_t i = 0; i < samples.size() && int(i) < capacity; ++i) {
+    const mgs::TuneSample& t = samples[i];
+    out[i] = mgs_tune_sample{t.key_bytes, t.size_class, t.n, t.variant.shape, t.variant.mode, t.ms, t.chosen ? 1 : 0};
+  }
+  if (count) *count = int(samples.size());
   mgs::clear_last_error();
   return MGS_OK;
 }

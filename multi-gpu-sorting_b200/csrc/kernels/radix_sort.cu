@@ -25,6 +25,7 @@
 //                        into the caller's buffer; reports device status words.
 // Algorithmic HBM traffic: n*w*(2P+1) bytes (+ n*w*2 for an odd pass count).
 #include <algorithm>
+#include <atomic>
 #include <cstdlib>
 #include <mutex>
 
@@ -904,23 +905,77 @@ struct RadixLayout {
   size_t num_tiles, status_bytes;
 };
 
-// Onesweep shape and multisplit strategy; the MGS_ONESWEEP_SHAPE and
-// MGS_RANK_MODE environment variables select alternatives for measurements.
-int onesweep_shape() {
-  static int shape = [] {
-    const char* e = getenv("MGS_ONESWEEP_SHAPE");
-    return (e && e[0] >= '0' && e[0] < '0' + kNumShapes) ? e[0] - '0' : kDefaultShape;
-  }();
-  return shape;
+// ---------------------------------------------------------------- variants --
+// Onesweep variant (tile shape x ranking mode) per key width and size class.
+// The table starts at shape 5 with ranking mode 3 everywhere, is replaced by a
+// tuning file when one is found (load_default_tuning, on first use), and can be
+// set or measured at run time (set_sort_variant, autotune). The
+// MGS_ONESWEEP_SHAPE / MGS_RANK_MODE environment variables override the table
+// for experiments.
+constexpr int kDefaultRankMode = 3;
+std::atomic<int> g_variant[2][kSizeClasses];  // shape * 10 + mode; 0 = not set
+
+int env_override(const char* name, int lo, int hi) {
+  const char* e = getenv(name);
+  return (e && e[0] >= '0' + lo && e[0] <= '0' + hi && e[1] == 0) ? e[0] - '0' : -1;
 }
 
-int rank_mode() {
-  static int mode = [] {
-    const char* e = getenv("MGS_RANK_MODE");
-    return (e && e[0] >= '0' && e[0] <= '4') ? e[0] - '0' : 3;
-  }();
-  return mode;
+}  // namespace
+
+int size_class(size_t n) {
+  if (n < (size_t(1) << 16)) return 0;
+  if (n < (size_t(1) << 18)) return 1;
+  if (n < (size_t(1) << 20)) return 2;
+  if (n < (size_t(1) << 22)) return 3;
+  if (n < (size_t(1) << 26)) return 4;
+  return 5;
 }
+
+size_t size_class_sample(int c) {
+  static const size_t sample[kSizeClasses] = {3u << 14, 3u << 16, 3u << 18, 3u << 20, size_t(1) << 24,
+                                              size_t(1) << 28};
+  return sample[c < 0 ? 0 : (c >= kSizeClasses ? kSizeClasses - 1 : c)];
+}
+
+bool valid_variant(SortVariant v) {
+  return v.shape >= 0 && v.shape < kNumShapes && (v.mode == 2 || v.mode == 3);
+}
+
+void ensure_default_tuning() {
+  static std::once_flag once;
+  std::call_once(once, [] { load_default_tuning(); });
+}
+
+bool store_sort_variant(int key_bytes, int size_class_index, SortVariant v) {
+  if ((key_bytes != 4 && key_bytes != 8) || size_class_index < 0 || size_class_index >= kSizeClasses ||
+      !valid_variant(v))
+    return false;
+  g_variant[key_bytes == 8][size_class_index].store(v.shape * 10 + v.mode, std::memory_order_relaxed);
+  return true;
+}
+
+bool set_sort_variant(int key_bytes, int size_class_index, SortVariant v) {
+  ensure_default_tuning();  // the default file must not overwrite this entry later
+  return store_sort_variant(key_bytes, size_class_index, v);
+}
+
+SortVariant table_variant(int key_bytes, int size_class_index) {
+  ensure_default_tuning();
+  const int c = size_class_index < 0 ? 0 : (size_class_index >= kSizeClasses ? kSizeClasses - 1 : size_class_index);
+  const int code = g_variant[key_bytes == 8][c].load(std::memory_order_relaxed);
+  return code ? SortVariant{code / 10, code % 10} : SortVariant{kDefaultShape, kDefaultRankMode};
+}
+
+SortVariant sort_variant(int key_bytes, size_t n) {
+  static const int env_shape = env_override("MGS_ONESWEEP_SHAPE", 0, kNumShapes - 1);
+  static const int env_mode = env_override("MGS_RANK_MODE", 2, 3);
+  SortVariant v = table_variant(key_bytes, size_class(n));
+  if (env_shape >= 0) v.shape = env_shape;
+  if (env_mode >= 0) v.mode = env_mode;
+  return v;
+}
+
+namespace {
 
 template <int KEY_BYTES, int SHAPE>
 constexpr size_t shape_tile() {
@@ -932,7 +987,7 @@ RadixLayout radix_layout(size_t n) {
   constexpr int w = int(sizeof(typename Tr::Bits));
   constexpr size_t tiles[kNumShapes] = {shape_tile<w, 0>(), shape_tile<w, 1>(), shape_tile<w, 2>(), shape_tile<w, 3>(),
                                          shape_tile<w, 4>(), shape_tile<w, 5>(), shape_tile<w, 6>()};
-  const size_t tile = tiles[onesweep_shape()];
+  const size_t tile = tiles[sort_variant(w, n).shape];
   // The look-back arrays are sized for the smallest tile, so every shape fits.
   constexpr size_t min_tile = shape_tile<w, 1>();
   RadixLayout L;
@@ -989,26 +1044,22 @@ cudaError_t launch_onesweep_variant(typename Tr::Bits* keys, typename Tr::Bits* 
                                     const RadixLayout& L, uint32_t n, bool use_tma, cudaStream_t stream,
                                     LaunchRecorder* rec) {
 #define MGS_LAUNCH(S, M) launch_onesweep_passes<Tr, S, StatusT, M>(keys, tmp, st, tbase, L, n, use_tma, stream, rec)
-  const int mode = rank_mode();
-  if (mode == 0) return MGS_LAUNCH(kDefaultShape, 0);
-  if (mode == 1) return MGS_LAUNCH(kDefaultShape, 1);
-  if (mode == 4) return MGS_LAUNCH(kDefaultShape, 4);
-  if (mode == 3) {
-    switch (onesweep_shape()) {
-      case 4: return MGS_LAUNCH(4, 3);
-      case 6: return MGS_LAUNCH(6, 3);
-      default: return MGS_LAUNCH(kDefaultShape, 3);
-    }
+#define MGS_SHAPES(M)                \
+  switch (v.shape) {                 \
+    case 0: return MGS_LAUNCH(0, M); \
+    case 1: return MGS_LAUNCH(1, M); \
+    case 2: return MGS_LAUNCH(2, M); \
+    case 3: return MGS_LAUNCH(3, M); \
+    case 4: return MGS_LAUNCH(4, M); \
+    case 6: return MGS_LAUNCH(6, M); \
+    default: return MGS_LAUNCH(5, M); \
   }
-  switch (onesweep_shape()) {
-    case 0: return MGS_LAUNCH(0, 2);
-    case 1: return MGS_LAUNCH(1, 2);
-    case 3: return MGS_LAUNCH(3, 2);
-    case 4: return MGS_LAUNCH(4, 2);
-    case 5: return MGS_LAUNCH(5, 2);
-    case 6: return MGS_LAUNCH(6, 2);
-    default: return MGS_LAUNCH(2, 2);
-  }
+  // The same choice as radix_layout made for this n (the table is read once per sort there and here;
+  // set_sort_variant must not run while sorts are being issued).
+  const SortVariant v = sort_variant(int(sizeof(typename Tr::Bits)), n);
+  if (v.mode == 2) MGS_SHAPES(2)
+  MGS_SHAPES(3)
+#undef MGS_SHAPES
 #undef MGS_LAUNCH
 }
 

@@ -7,6 +7,8 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#include <vector>
+
 #include "launch.cuh"
 
 namespace mgs {
@@ -34,5 +36,48 @@ cudaError_t segmented_sort(int dtype, void* d_keys, size_t n, const uint64_t* d_
 
 // Number of kernel launches radix_sort issues for (dtype, n).
 int radix_sort_launches(int dtype, size_t n);
+
+// Onesweep variant choice. Key widths 4 and 8 bytes each have a table of
+// kSizeClasses entries (size_class: n < 2^16, < 2^18, < 2^20, < 2^22, < 2^26,
+// larger); each entry names a tile shape (0..6: threads x keys per thread, see
+// OnesweepShape) and a ranking mode (2: shared-memory peer masks, 3: ballots
+// for half of the items). radix_sort reads the entry of its (width, n).
+constexpr int kSizeClasses = 6;
+struct SortVariant {
+  int shape;
+  int mode;
+};
+int size_class(size_t n);
+size_t size_class_sample(int size_class);  // the key count the autotuner times for a class
+bool valid_variant(SortVariant v);
+bool set_sort_variant(int key_bytes, int size_class, SortVariant v);  // false when out of range
+SortVariant sort_variant(int key_bytes, size_t n);  // the table's entry, then the environment overrides
+SortVariant table_variant(int key_bytes, int size_class);  // the table's entry alone
+// Tuning files (format in tune.cu): load returns the number of entries read,
+// -1 when the file cannot be opened, -2 when a line is malformed (valid lines
+// before and after it are still applied); save writes the whole table.
+int load_tuning_file(const char* path);
+bool save_tuning_file(const char* path);
+// The default tuning file (the MGS_TUNE_FILE path, else tuning/b200.tune
+// beside the library's own directory) is read once, before the table is first
+// read or set: ensure_default_tuning runs load_default_tuning on that first use.
+// store_sort_variant writes an entry without that step (file reading uses it).
+void ensure_default_tuning();
+void load_default_tuning();
+bool store_sort_variant(int key_bytes, int size_class, SortVariant v);
+
+// Autotuner: for each size class whose sample size is at most max_n, times every
+// variant (CUDA events, median of `reps` sorts of uniformly random keys of the
+// dtype's width) and stores the fastest in the table. Allocates its own device
+// buffers (keys, a pristine copy, scratch) and frees them. Sorts must not be
+// issued from other threads meanwhile. Synchronous.
+struct TuneSample {
+  int key_bytes, size_class;
+  size_t n;
+  SortVariant variant;
+  double ms;
+  bool chosen;
+};
+cudaError_t autotune(int dtype, size_t max_n, int reps, std::vector<TuneSample>* out);
 
 }  // namespace mgs

@@ -63,6 +63,11 @@ class ServerStats(ctypes.Structure):
                 ("busy_s", ctypes.c_double)]
 
 
+class TuneSample(ctypes.Structure):
+    _fields_ = [("key_bytes", ctypes.c_int), ("size_class", ctypes.c_int), ("n", ctypes.c_size_t),
+                ("shape", ctypes.c_int), ("rank_mode", ctypes.c_int), ("ms", ctypes.c_double), ("chosen", ctypes.c_int)]
+
+
 class KernelTime(ctypes.Structure):
     _fields_ = [("name", ctypes.c_char * 48), ("launches", ctypes.c_uint64), ("total_ms", ctypes.c_double)]
 
@@ -122,6 +127,12 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "mgs_plan_launch": ([c_void, c_void], c_int),
         "mgs_plan_launch_count": ([c_void, ctypes.POINTER(ctypes.c_uint64)], c_int),
         "mgs_plan_destroy": ([c_void], c_int),
+        "mgs_tune_get": ([c_int, c_size, ctypes.POINTER(c_int), ctypes.POINTER(c_int)], c_int),
+        "mgs_tune_set": ([c_int, c_int, c_int, c_int], c_int),
+        "mgs_tune_load": ([ctypes.c_char_p], c_int),
+        "mgs_tune_save": ([ctypes.c_char_p], c_int),
+        "mgs_autotune": ([c_void, c_int, c_size, c_int, ctypes.POINTER(TuneSample), c_int, ctypes.POINTER(c_int)],
+                         c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -182,6 +193,29 @@ def generate(dtype, distribution: str, seed: int, n: int, out: np.ndarray | None
     _check(lib.mgs_generate(dtype_code(dtype), distribution.encode(), int(seed) & 0xFFFFFFFF,
                             out.ctypes.data_as(ctypes.c_void_p), int(n)))
     return out
+
+
+def tune_get(dtype, n: int) -> tuple:
+    """(shape, rank_mode) the radix sort uses for n keys of this dtype (mgs_tune_get)."""
+    lib = load_library()
+    shape, mode = ctypes.c_int(), ctypes.c_int()
+    _check(lib.mgs_tune_get(dtype_code(dtype), int(n), ctypes.byref(shape), ctypes.byref(mode)))
+    return shape.value, mode.value
+
+
+def tune_set(dtype, size_class: int, shape: int, rank_mode: int) -> None:
+    lib = load_library()
+    _check(lib.mgs_tune_set(dtype_code(dtype), int(size_class), int(shape), int(rank_mode)))
+
+
+def tune_load(path: str) -> None:
+    lib = load_library()
+    _check(lib.mgs_tune_load(path.encode()))
+
+
+def tune_save(path: str) -> None:
+    lib = load_library()
+    _check(lib.mgs_tune_save(path.encode()))
 
 
 def sort_device_noalloc(d_keys: int, n: int, dtype, stream: int = 0) -> None:
@@ -332,6 +366,16 @@ class Context:
                                                    ctypes.c_void_p(d_offsets), int(num_segments),
                                                    ctypes.c_void_p(d_temp or None), int(temp_bytes),
                                                    ctypes.c_void_p(stream or None)))
+
+    # --- autotuner ---
+    def autotune(self, dtype, max_n: int, reps: int = 3) -> list:
+        """Times every onesweep variant per size class up to max_n and keeps the fastest (mgs_autotune)."""
+        cap = 256
+        arr = (TuneSample * cap)()
+        cnt = ctypes.c_int()
+        _check(self._lib.mgs_autotune(self.handle, dtype_code(dtype), int(max_n), int(reps), arr, cap,
+                                      ctypes.byref(cnt)))
+        return [{f: getattr(arr[i], f) for f, _ in TuneSample._fields_} for i in range(min(cnt.value, cap))]
 
     # --- recorded sorts (CUDA graphs) ---
     def plan_sort(self, d_keys: int, n: int, dtype, d_temp: int = 0, temp_bytes: int = 0) -> "Plan":
