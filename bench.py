@@ -532,6 +532,52 @@ def sweep_merge(mgs, torch, n, reps=3):
     ctx.close()
 
 
+def sweep_pairs(mgs, torch, reps=3):
+    """Key-value sort (thrust::sort_by_key order) on device-resident data: 2^30 u32 keys with u32 values and 2^29
+    u64 keys with u64 values; the values are the input positions, so the result is checked by gathering the input
+    through them (ascending, a permutation, equal keys in input order). Algorithmic bytes: every pass reads and
+    writes keys and values, plus one histogram read of the keys."""
+    ctx = mgs.Context(0)
+    peak, _ = measured_hbm_peak()
+    stream = torch.cuda.Stream()
+    for dtype, n, vb in (("u32", 1 << 30, 4), ("u64", 1 << 29, 8)):
+        w = 4 if dtype == "u32" else 8
+        st = torch.int32 if w == 4 else torch.int64
+        vt = torch.int32 if vb == 4 else torch.int64
+        src = torch.from_numpy(mgs.generate(dtype, "full-uniform", SEED, n).view(np.int32 if w == 4 else np.int64)).cuda()
+        keys, vals = torch.empty_like(src), torch.empty(n, dtype=vt, device="cuda")
+        iota = torch.arange(n, dtype=vt, device="cuda")
+        temp_bytes = mgs.Context.sort_pairs_temp_bytes(dtype, vb, n)
+        temp = torch.empty(temp_bytes, dtype=torch.uint8, device="cuda")
+        times = []
+        for i in range(reps + 1):
+            with torch.cuda.stream(stream):
+                keys.copy_(src)
+                vals.copy_(iota)
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                ctx.sort_pairs_device(keys.data_ptr(), vals.data_ptr(), vb, n, dtype, temp.data_ptr(), temp_bytes,
+                                      stream.cuda_stream)
+                b.record(stream)
+            stream.synchronize()
+            if i > 0:
+                times.append(a.elapsed_time(b))
+        ctx.synchronize()
+        idx = vals.to(torch.int64)
+        k = order_key(torch, keys, dtype)
+        ok = bool(torch.equal(src[idx], keys)) and bool((k[1:] >= k[:-1]).all())
+        same = k[1:] == k[:-1]
+        ok = ok and bool((idx[1:][same] > idx[:-1][same]).all())
+        ok = ok and bool(torch.equal(torch.sort(idx)[0], torch.arange(n, device="cuda")))
+        ms = statistics.median(times)
+        alg = n * (2 * w * (w + vb) + w)
+        print(json.dumps({"sweep": "pairs", "dtype": dtype, "value_bytes": vb, "n": n, "ms": ms,
+                          "pairs_per_s": n / (ms / 1e3), "hbm_alg_gbs": alg / (ms / 1e3) / 1e9,
+                          "roofline_frac": alg / (ms / 1e3) / 1e9 / peak, "verified": ok}), flush=True)
+        del src, keys, vals, iota, temp, idx, k, same
+    ctx.close()
+
+
 def sweep_tune(mgs, out_path, max_n=1 << 28, reps=3):
     """Autotuner run: every onesweep variant (7 tile shapes x 2 ranking modes) timed per size class up to max_n
     for 4- and 8-byte keys; the fastest per class goes into the table, which is written to out_path if given."""
@@ -671,7 +717,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched (segmented) measurement")
     ap.add_argument("--no-served", action="store_true", help="skip the serving-loop measurement")
-    ap.add_argument("--sweep", choices=["types", "merge", "ooc", "tune"],
+    ap.add_argument("--sweep", choices=["types", "merge", "ooc", "tune", "pairs"],
                     help="measure another workload of the sort API instead (one JSON line per case)")
     ap.add_argument("--sweep-n", type=int, default=0, help="keys per case of --sweep (0: the workload's default)")
     ap.add_argument("--tune-out", default="", help="--sweep tune: write the tuned variant table to this file")
@@ -691,6 +737,8 @@ def main():
         mgs = load_mgs()
         if args.sweep == "types":
             sweep_types(mgs, torch, args.sweep_n or N_KEYS)
+        elif args.sweep == "pairs":
+            sweep_pairs(mgs, torch)
         elif args.sweep == "tune":
             sweep_tune(mgs, args.tune_out, args.sweep_n or (1 << 28))
         elif args.sweep == "merge":

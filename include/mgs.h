@@ -175,6 +175,21 @@ int mgs_segmented_sort_temp_bytes(int dtype, size_t n, size_t num_segments, size
 int mgs_segmented_sort_device(mgs_ctx* ctx, int dtype, void* d_keys, size_t n, const uint64_t* d_offsets,
                               size_t num_segments, void* d_temp, size_t temp_bytes, void* stream);
 
+/* ---- key-value sort and argsort ---------------------------------------------
+ * Not in the reference, whose sorts carry keys only; this is the
+ * thrust::sort_by_key form of the library it sorts with (src/tanasic_sort.cuh:264):
+ * d_keys[0..n) sorted exactly as mgs_sort_device sorts them (stable), and
+ * d_values[0..n) (value_bytes = 4 or 8 per key; any payload: row ids, pointers,
+ * indices) moved with their keys, so values of equal keys keep their input
+ * order. mgs_argsort_device writes into d_indices the input position of each
+ * key in sorted order (index_bytes = 4 or 8) and sorts the keys in place.
+ * Scratch as for mgs_sort_device (NULL: the context's arena). Asynchronous. */
+int mgs_sort_pairs_temp_bytes(int dtype, size_t value_bytes, size_t n, size_t* bytes);
+int mgs_sort_pairs_device(mgs_ctx* ctx, int dtype, void* d_keys, void* d_values, size_t value_bytes, size_t n,
+                          void* d_temp, size_t temp_bytes, void* stream);
+int mgs_argsort_device(mgs_ctx* ctx, int dtype, void* d_keys, void* d_indices, size_t index_bytes, size_t n,
+                       void* d_temp, size_t temp_bytes, void* stream);
+
 /* ---- recorded sorts (CUDA graphs) -------------------------------------------
  * No counterpart in the reference (its sorts are host-driven thrust calls). A
  * plan records once, into a CUDA graph, the launches of one device sort or one

@@ -338,6 +338,75 @@ int mgs_sort_device(mgs_ctx* ctx, int dtype, void* d_keys, size_t n, void* d_tem
   return MGS_OK;
 }
 
+int mgs_sort_pairs_temp_bytes(int dtype, size_t value_bytes, size_t n, size_t* bytes) {
+  if (!bytes) return invalid("mgs_sort_pairs_temp_bytes: bytes is null");
+  if (mgs::dtype_bytes(dtype) == 0) return invalid("mgs_sort_pairs_temp_bytes: unknown dtype");
+  if (value_bytes != 4 && value_bytes != 8) return invalid("mgs_sort_pairs_temp_bytes: value_bytes must be 4 or 8");
+  *bytes = n ? mgs::radix_sort_pairs_temp_bytes(dtype, value_bytes, n) : 0;
+  return MGS_OK;
+}
+
+// Shared argument checks and scratch choice of the key-value entry points.
+static int pairs_call(mgs_ctx* ctx, const char* what, int dtype, void* d_keys, void* d_values, size_t value_bytes,
+                      size_t n, void* d_temp, size_t temp_bytes, void* stream, bool argsort) {
+  if (!ctx) return invalid("key-value sort: ctx is null");
+  const size_t w = mgs::dtype_bytes(dtype);
+  if (w == 0) {
+    set_last_error("%s: unknown dtype", what);
+    return MGS_ERR_INVALID;
+  }
+  if (value_bytes != 4 && value_bytes != 8) {
+    set_last_error("%s: value_bytes must be 4 or 8", what);
+    return MGS_ERR_INVALID;
+  }
+  if (n == 0) return MGS_OK;
+  if (!d_keys || !d_values) {
+    set_last_error("%s: null pointer", what);
+    return MGS_ERR_INVALID;
+  }
+  if (reinterpret_cast<uintptr_t>(d_keys) % w != 0 || reinterpret_cast<uintptr_t>(d_values) % value_bytes != 0) {
+    set_last_error("%s: keys or values are not aligned to their size", what);
+    return MGS_ERR_INVALID;
+  }
+  if (n > kMaxDeviceSortKeys) {
+    set_last_error("%s: n must be below 2^32", what);
+    return MGS_ERR_INVALID;
+  }
+  Context& c = ctx->impl;
+  DeviceGuard g(c.device);
+  const size_t need = mgs::radix_sort_pairs_temp_bytes(dtype, value_bytes, n);
+  if (d_temp == nullptr) {
+    cudaError_t e = c.reserve(need);
+    if (e != cudaSuccess) return cuda_fail(e, what);
+    d_temp = c.arena;
+    temp_bytes = c.arena_bytes;
+  } else if (temp_bytes < need) {
+    set_last_error("%s: d_temp holds %zu bytes, %zu needed", what, temp_bytes, need);
+    return MGS_ERR_INVALID;
+  }
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c.compute;
+  const cudaError_t e =
+      argsort ? mgs::radix_argsort(dtype, d_keys, d_values, value_bytes, n, d_temp, temp_bytes, s, c.d_status,
+                                   &c.recorder)
+              : mgs::radix_sort_pairs(dtype, d_keys, d_values, value_bytes, n, d_temp, temp_bytes, s, c.d_status,
+                                      &c.recorder);
+  if (e != cudaSuccess) return cuda_fail(e, what);
+  mgs::clear_last_error();
+  return MGS_OK;
+}
+
+int mgs_sort_pairs_device(mgs_ctx* ctx, int dtype, void* d_keys, void* d_values, size_t value_bytes, size_t n,
+                          void* d_temp, size_t temp_bytes, void* stream) {
+  return pairs_call(ctx, "mgs_sort_pairs_device", dtype, d_keys, d_values, value_bytes, n, d_temp, temp_bytes, stream,
+                    false);
+}
+
+int mgs_argsort_device(mgs_ctx* ctx, int dtype, void* d_keys, void* d_indices, size_t index_bytes, size_t n,
+                       void* d_temp, size_t temp_bytes, void* stream) {
+  return pairs_call(ctx, "mgs_argsort_device", dtype, d_keys, d_indices, index_bytes, n, d_temp, temp_bytes, stream,
+                    true);
+}
+
 int mgs_sort_host(mgs_ctx* ctx, int dtype, void* h_keys, size_t n) {
   if (!ctx) return invalid("mgs_sort_host: ctx is null");
   const size_t w = mgs::dtype_bytes(dtype);

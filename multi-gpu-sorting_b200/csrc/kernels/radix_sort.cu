@@ -28,6 +28,7 @@
 #include <atomic>
 #include <cstdlib>
 #include <mutex>
+#include <type_traits>
 
 #include "device_common.cuh"
 #include "dispatch.cuh"
@@ -209,12 +210,26 @@ __global__ __launch_bounds__(kRadix) void radix_scan_kernel(RadixState* __restri
 }
 
 // ---------------------------------------------------------------- K2 --------
-template <class Tr, int BLOCK, int ITEMS, int CHAINS>
+// Value payload of a key-value sort (uint32_t or unsigned long long, opaque
+// to the sort); NoValue for a keys-only sort, for which every value step below
+// compiles to nothing.
+struct NoValue {};
+template <typename V>
+constexpr bool kHasValues = !std::is_same<V, NoValue>::value;
+template <typename V, int N>
+struct ValueTiles {
+  alignas(16) V v[2][N];  // the values of the two key buffers
+};
+template <int N>
+struct ValueTiles<NoValue, N> {};
+
+template <class Tr, int BLOCK, int ITEMS, int CHAINS, typename V = NoValue>
 struct OnesweepSmem {
   static constexpr int kTile = BLOCK * ITEMS;
   static constexpr int kWarps = BLOCK / 32;
   static constexpr int kChains = kWarps * CHAINS;  // ranking chains (CHAINS per warp)
   typename Tr::Bits keys[2][kTile];    // double buffer: tile being sorted / next tile in flight
+  ValueTiles<V, kTile> vals;
   uint32_t ccount[kChains * kRadix];     // per-chain digit counters -> tile positions
   uint32_t masks[kChains * 2 * kRadix];  // per-chain peer masks (shared-memory multisplit)
   uint32_t tile_start[kRadix];           // exclusive scan of the tile's digit counts
@@ -282,11 +297,14 @@ __device__ __forceinline__ uint32_t digit_peers(uint32_t d, bool ok, uint32_t* m
 // (count = the tile's count of digit tid for tid < 256): warps that do extra
 // work there rank later, while the other warps rank at once. The caller
 // synchronizes before reading dst.
-template <class Tr, int BLOCK, int ITEMS, int CHAINS, int MATCH, bool FULL, bool ALLOW_SKIP, class OnCounts,
+// With values, src_val/dst_val are the value buffers of src/dst: every value
+// goes to the slot its key goes to.
+template <class Tr, int BLOCK, int ITEMS, int CHAINS, int MATCH, bool FULL, bool ALLOW_SKIP, typename V, class OnCounts,
           class Between>
-__device__ __forceinline__ bool rank_tile(OnesweepSmem<Tr, BLOCK, ITEMS, CHAINS>& sm, const typename Tr::Bits* src,
+__device__ __forceinline__ bool rank_tile(OnesweepSmem<Tr, BLOCK, ITEMS, CHAINS, V>& sm, const typename Tr::Bits* src,
                                           typename Tr::Bits* dst, uint32_t valid, int pass, uint32_t* tile_count_out,
-                                          OnCounts on_counts, Between between) {
+                                          OnCounts on_counts, Between between, const V* src_val = nullptr,
+                                          V* dst_val = nullptr) {
   using Bits = typename Tr::Bits;
   constexpr int kTile = BLOCK * ITEMS;
   constexpr int kChains = (BLOCK / 32) * CHAINS;
@@ -300,10 +318,12 @@ __device__ __forceinline__ bool rank_tile(OnesweepSmem<Tr, BLOCK, ITEMS, CHAINS>
   __syncthreads();
   // Phase 1: per-chain digit counts.
   Bits key[ITEMS];
+  V val[kHasValues<V> ? ITEMS : 1];
 #pragma unroll
   for (int i = 0; i < ITEMS; ++i) {
     const uint32_t idx = wbase + i * 32 + lane;
     key[i] = src[idx];
+    if constexpr (kHasValues<V>) val[i] = src_val[idx];
     uint32_t* cc = sm.ccount + (warp * CHAINS + i / kPerChain) * kRadix;
     if (FULL || idx < valid) atomicAdd(&cc[Tr::Digit(key[i], pass)], 1u);
   }
@@ -380,8 +400,12 @@ __device__ __forceinline__ bool rank_tile(OnesweepSmem<Tr, BLOCK, ITEMS, CHAINS>
     // counter updates before its counter reads; ballots and match need one here.
     if (MATCH < 2) __syncwarp();
 #pragma unroll
-    for (int h = 0; h < CHAINS; ++h)
-      if (ok[h] && pos[h] < uint32_t(kTile)) dst[pos[h]] = key[h * kPerChain + j];
+    for (int h = 0; h < CHAINS; ++h) {
+      if (ok[h] && pos[h] < uint32_t(kTile)) {
+        dst[pos[h]] = key[h * kPerChain + j];
+        if constexpr (kHasValues<V>) dst_val[pos[h]] = val[h * kPerChain + j];
+      }
+    }
   }
   return false;
 }
@@ -398,13 +422,22 @@ struct alignas(16) TileSpan {
   const uint32_t* bucket;        // 256 bucket starts of this pass within the segment
 };
 
+// Where a key-value sort's values come from and go to (the whole array).
+template <typename V>
+struct ValueSpan {
+  const V* src;
+  V* dst;
+};
+
 // One tile: count digits in shared memory (publishing the tile's counts for
 // the look-back as soon as they are known), look back over the segment's
-// earlier tiles while the other warps rank, scatter the digit runs.
-template <class Tr, int BLOCK, int ITEMS, int CHAINS, typename StatusT, int MATCH, bool FULL>
-__device__ __forceinline__ void onesweep_tile(OnesweepSmem<Tr, BLOCK, ITEMS, CHAINS>& sm, typename Tr::Bits* skeys,
+// earlier tiles while the other warps rank, scatter the digit runs (with their
+// values, svals being the tile's value buffer, when V is a value type).
+template <class Tr, int BLOCK, int ITEMS, int CHAINS, typename StatusT, int MATCH, bool FULL, typename V>
+__device__ __forceinline__ void onesweep_tile(OnesweepSmem<Tr, BLOCK, ITEMS, CHAINS, V>& sm, typename Tr::Bits* skeys,
                                               RadixState* __restrict__ st, StatusT* __restrict__ lb_cur,
-                                              const TileSpan<Tr>& span, uint32_t tile, uint32_t valid, int pass) {
+                                              const TileSpan<Tr>& span, uint32_t tile, uint32_t valid, int pass,
+                                              V* svals, const ValueSpan<V>& vspan) {
   using Bits = typename Tr::Bits;
   using LW = LookbackWord<StatusT>;
   const int tid = threadIdx.x;
@@ -460,7 +493,8 @@ __device__ __forceinline__ void onesweep_tile(OnesweepSmem<Tr, BLOCK, ITEMS, CHA
           LW::store(lb_cur + size_t(tile) * kRadix + tid, LW::kPrefix | (excl + count));
         }
         sm.gbase[tid] = span.bucket[tid] + uint32_t(excl) - sm.tile_start[tid];
-      });
+      },
+      svals, svals);
   __syncthreads();
 
   // Phase 3: consecutive threads write consecutive positions of one digit run.
@@ -471,7 +505,10 @@ __device__ __forceinline__ void onesweep_tile(OnesweepSmem<Tr, BLOCK, ITEMS, CHA
     if (FULL || idx < valid) {
       const Bits k = skeys[idx];
       const uint32_t gpos = sm.gbase[Tr::Digit(k, pass)] + idx;
-      if (gpos < span.seg_len) span.dst[gpos] = k;
+      if (gpos < span.seg_len) {
+        span.dst[gpos] = k;
+        if constexpr (kHasValues<V>) vspan.dst[gpos] = svals[idx];
+      }
     }
   }
 }
@@ -505,18 +542,22 @@ __device__ __forceinline__ TileSpan<Tr> seg_span(const SegLarge& sg, const typen
   return sp;
 }
 
-template <class Tr, int BLOCK, int ITEMS, int MINB, int CHAINS, typename StatusT, int MATCH, bool SEG>
+// vbuf0/vbuf1: the value buffers of buf0/buf1 (key-value sort), else null.
+template <class Tr, int BLOCK, int ITEMS, int MINB, int CHAINS, typename StatusT, int MATCH, bool SEG,
+          typename V = NoValue>
 __global__ __launch_bounds__(BLOCK, MINB) void radix_onesweep_kernel(typename Tr::Bits* buf0, typename Tr::Bits* buf1,
                                                                      RadixState* __restrict__ st,
                                                                      StatusT* __restrict__ lb_cur,
                                                                      StatusT* __restrict__ lb_next, uint32_t n,
                                                                      uint32_t num_tiles_arg, int pass, int use_tma,
-                                                                     SegLarge sg) {
+                                                                     SegLarge sg, V* vbuf0, V* vbuf1) {
   using Bits = typename Tr::Bits;
-  using Smem = OnesweepSmem<Tr, BLOCK, ITEMS, CHAINS>;
+  using Smem = OnesweepSmem<Tr, BLOCK, ITEMS, CHAINS, V>;
+  static_assert(!(SEG && kHasValues<V>), "the segmented sort carries no values");
   constexpr int kTile = Smem::kTile;
   constexpr int kChains = Smem::kChains;
-  constexpr uint32_t kTileBytes = uint32_t(kTile * sizeof(Bits));
+  constexpr uint32_t kKeyBytes = uint32_t(kTile * sizeof(Bits));
+  constexpr uint32_t kTileBytes = kKeyBytes + (kHasValues<V> ? uint32_t(kTile * sizeof(V)) : 0u);
   static_assert(BLOCK >= kRadix, "one thread per digit");
   extern __shared__ __align__(128) unsigned char smem_raw[];
   Smem& sm = *reinterpret_cast<Smem*>(smem_raw);
@@ -533,6 +574,7 @@ __global__ __launch_bounds__(BLOCK, MINB) void radix_onesweep_kernel(typename Tr
   for (int q = 0; q < pass; ++q) sel ^= (st->skip[q] == 0u) ? 1 : 0;
   const Bits* src = sel ? buf1 : buf0;
   Bits* dst = sel ? buf0 : buf1;
+  const ValueSpan<V> vspan{sel ? vbuf1 : vbuf0, sel ? vbuf0 : vbuf1};
 
   auto span_of = [&](uint32_t t) {
     if (SEG) return seg_span<Tr>(sg, src, dst, t, pass);
@@ -541,7 +583,17 @@ __global__ __launch_bounds__(BLOCK, MINB) void radix_onesweep_kernel(typename Tr
   };
   auto tma_ok = [&](const TileSpan<Tr>& sp, uint32_t t) {
     const size_t off = size_t(t - sp.first_tile) * kTile;
-    return use_tma && off + kTile <= sp.seg_len && ((reinterpret_cast<uintptr_t>(sp.src + off) & 15u) == 0);
+    bool ok = use_tma && off + kTile <= sp.seg_len && ((reinterpret_cast<uintptr_t>(sp.src + off) & 15u) == 0);
+    if constexpr (kHasValues<V>) ok = ok && ((reinterpret_cast<uintptr_t>(vspan.src + off) & 15u) == 0);
+    return ok;
+  };
+  // One tile's keys (and values) into buffer b with the TMA, completing on bar[b].
+  auto issue_copy = [&](int b, const TileSpan<Tr>& sp, uint32_t t) {
+    const size_t off = size_t(t - sp.first_tile) * kTile;
+    mbar_arrive_expect_tx(&sm.bar[b], kTileBytes);
+    bulk_copy_g2s(sm.keys[b], sp.src + off, kKeyBytes, &sm.bar[b]);
+    if constexpr (kHasValues<V>)
+      bulk_copy_g2s(sm.vals.v[b], vspan.src + off, uint32_t(kTile * sizeof(V)), &sm.bar[b]);
   };
 
   // Persistent CTA: tiles come in launch order from an atomic counter; the
@@ -562,10 +614,7 @@ __global__ __launch_bounds__(BLOCK, MINB) void radix_onesweep_kernel(typename Tr
     if (t < num_tiles) {
       const TileSpan<Tr> sp = span_of(t);
       spans[0] = sp;
-      if (tma_ok(sp, t)) {
-        mbar_arrive_expect_tx(&sm.bar[0], kTileBytes);
-        bulk_copy_g2s(sm.keys[0], sp.src + size_t(t - sp.first_tile) * kTile, kTileBytes, &sm.bar[0]);
-      }
+      if (tma_ok(sp, t)) issue_copy(0, sp, t);
     }
   }
   __syncthreads();
@@ -582,8 +631,7 @@ __global__ __launch_bounds__(BLOCK, MINB) void radix_onesweep_kernel(typename Tr
         spans[cur ^ 1] = sp;
         if (tma_ok(sp, t)) {
           asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-          mbar_arrive_expect_tx(&sm.bar[cur ^ 1], kTileBytes);
-          bulk_copy_g2s(sm.keys[cur ^ 1], sp.src + size_t(t - sp.first_tile) * kTile, kTileBytes, &sm.bar[cur ^ 1]);
+          issue_copy(cur ^ 1, sp, t);
         }
       }
     }
@@ -600,11 +648,17 @@ __global__ __launch_bounds__(BLOCK, MINB) void radix_onesweep_kernel(typename Tr
       }
     } else {
       for (uint32_t i = tid; i < valid; i += BLOCK) skeys[i] = span.src[base + i];
+      if constexpr (kHasValues<V>)
+        for (uint32_t i = tid; i < valid; i += BLOCK) sm.vals.v[cur][i] = vspan.src[base + i];
     }
+    V* svals = nullptr;
+    if constexpr (kHasValues<V>) svals = sm.vals.v[cur];
     if (valid == uint32_t(kTile)) {
-      onesweep_tile<Tr, BLOCK, ITEMS, CHAINS, StatusT, MATCH, true>(sm, skeys, st, lb_cur, span, tile, valid, pass);
+      onesweep_tile<Tr, BLOCK, ITEMS, CHAINS, StatusT, MATCH, true>(sm, skeys, st, lb_cur, span, tile, valid, pass,
+                                                                    svals, vspan);
     } else {
-      onesweep_tile<Tr, BLOCK, ITEMS, CHAINS, StatusT, MATCH, false>(sm, skeys, st, lb_cur, span, tile, valid, pass);
+      onesweep_tile<Tr, BLOCK, ITEMS, CHAINS, StatusT, MATCH, false>(sm, skeys, st, lb_cur, span, tile, valid, pass,
+                                                                     svals, vspan);
     }
     __syncthreads();
     cur ^= 1;
@@ -871,22 +925,22 @@ __global__ __launch_bounds__(kRadix) void seg_scan_kernel(const uint32_t* __rest
 }
 
 // ---------------------------------------------------------------- K3 --------
-template <class Tr>
-__global__ __launch_bounds__(256) void radix_finalize_kernel(typename Tr::Bits* __restrict__ buf0,
-                                                             const typename Tr::Bits* __restrict__ buf1,
-                                                             const RadixState* __restrict__ st, uint32_t n,
-                                                             uint32_t* __restrict__ d_status) {
-  using Bits = typename Tr::Bits;
+// Copies buf1 back into buf0 when an odd number of passes ran (the sorted data
+// then sits in the ping-pong buffer); reports the sort's status word.
+template <int P, typename T>
+__device__ __forceinline__ void copy_back_if_odd(T* __restrict__ buf0, const T* __restrict__ buf1,
+                                                 const RadixState* __restrict__ st, uint32_t n,
+                                                 uint32_t* __restrict__ d_status) {
   int live = 0;
 #pragma unroll
-  for (int p = 0; p < Tr::kPasses; ++p) live += (st->skip[p] == 0u) ? 1 : 0;
+  for (int p = 0; p < P; ++p) live += (st->skip[p] == 0u) ? 1 : 0;
   if (blockIdx.x == 0 && threadIdx.x == 0 && d_status != nullptr && st->error != 0u) atomicOr(d_status, st->error);
   if ((live & 1) == 0) return;
   const size_t gtid = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
   const size_t gstride = size_t(gridDim.x) * blockDim.x;
   const bool aligned = ((reinterpret_cast<uintptr_t>(buf0) | reinterpret_cast<uintptr_t>(buf1)) & 15u) == 0;
   if (aligned) {
-    constexpr int kPerVec = 16 / int(sizeof(Bits));
+    constexpr int kPerVec = 16 / int(sizeof(T));
     const size_t nvec = n / kPerVec;
     const uint4* s = reinterpret_cast<const uint4*>(buf1);
     uint4* d = reinterpret_cast<uint4*>(buf0);
@@ -897,11 +951,30 @@ __global__ __launch_bounds__(256) void radix_finalize_kernel(typename Tr::Bits* 
   }
 }
 
+template <class Tr>
+__global__ __launch_bounds__(256) void radix_finalize_kernel(typename Tr::Bits* __restrict__ buf0,
+                                                             const typename Tr::Bits* __restrict__ buf1,
+                                                             const RadixState* __restrict__ st, uint32_t n,
+                                                             uint32_t* __restrict__ d_status) {
+  copy_back_if_odd<Tr::kPasses>(buf0, buf1, st, n, d_status);
+}
+
+// Key-value sort: the keys and the values go back when an odd number of passes ran.
+template <class Tr, typename V>
+__global__ __launch_bounds__(256) void radix_finalize_pairs_kernel(typename Tr::Bits* __restrict__ buf0,
+                                                                   const typename Tr::Bits* __restrict__ buf1,
+                                                                   V* __restrict__ vbuf0, const V* __restrict__ vbuf1,
+                                                                   const RadixState* __restrict__ st, uint32_t n,
+                                                                   uint32_t* __restrict__ d_status) {
+  copy_back_if_odd<Tr::kPasses>(buf0, buf1, st, n, d_status);
+  copy_back_if_odd<Tr::kPasses>(vbuf0, vbuf1, st, n, nullptr);
+}
+
 // ---------------------------------------------------------------- host ------
 size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
 struct RadixLayout {
-  size_t state_off, lb0_off, lb1_off, keys_off, total;
+  size_t state_off, lb0_off, lb1_off, keys_off, vals_off, total;
   size_t num_tiles, status_bytes;
 };
 
@@ -982,13 +1055,29 @@ constexpr size_t shape_tile() {
   return size_t(OnesweepShape<KEY_BYTES, SHAPE>::kBlock) * OnesweepShape<KEY_BYTES, SHAPE>::kItems;
 }
 
-template <class Tr>
+// Key-value tiles: 512 threads x kItems keys, sized so that two tiles of keys
+// and values fit in shared memory beside the per-warp counters and masks
+// (8-byte pairs: 16 keys per thread, 12-byte pairs: 12, 16-byte pairs: 8).
+template <int KEY_BYTES, int VALUE_BYTES>
+struct PairShape {
+  static constexpr int kBlock = 512;
+  static constexpr int kItems = (KEY_BYTES + VALUE_BYTES == 8) ? 16 : ((KEY_BYTES + VALUE_BYTES == 12) ? 12 : 8);
+  static constexpr int kMinBlocks = 1, kChains = 1;
+};
+
+template <class Tr, typename V = NoValue>
 RadixLayout radix_layout(size_t n) {
   constexpr int w = int(sizeof(typename Tr::Bits));
-  constexpr size_t tiles[kNumShapes] = {shape_tile<w, 0>(), shape_tile<w, 1>(), shape_tile<w, 2>(), shape_tile<w, 3>(),
-                                         shape_tile<w, 4>(), shape_tile<w, 5>(), shape_tile<w, 6>()};
-  const size_t tile = tiles[sort_variant(w, n).shape];
-  // The look-back arrays are sized for the smallest tile, so every shape fits.
+  size_t tile;
+  if constexpr (kHasValues<V>) {
+    tile = size_t(PairShape<w, int(sizeof(V))>::kBlock) * PairShape<w, int(sizeof(V))>::kItems;
+  } else {
+    constexpr size_t tiles[kNumShapes] = {shape_tile<w, 0>(), shape_tile<w, 1>(), shape_tile<w, 2>(),
+                                           shape_tile<w, 3>(), shape_tile<w, 4>(), shape_tile<w, 5>(),
+                                           shape_tile<w, 6>()};
+    tile = tiles[sort_variant(w, n).shape];
+  }
+  // The look-back arrays are sized for the smallest tile, so every shape (and the key-value tiles) fits.
   constexpr size_t min_tile = shape_tile<w, 1>();
   RadixLayout L;
   L.num_tiles = (n + tile - 1) / tile;
@@ -999,6 +1088,11 @@ RadixLayout radix_layout(size_t n) {
   L.lb1_off = L.lb0_off + align_up(lb_bytes, 256);
   L.keys_off = L.lb1_off + align_up(lb_bytes, 256);
   L.total = L.keys_off + align_up(n * sizeof(typename Tr::Bits), 256);
+  L.vals_off = 0;
+  if constexpr (kHasValues<V>) {
+    L.vals_off = L.total;
+    L.total += align_up(n * sizeof(V), 256);
+  }
   return L;
 }
 
@@ -1033,7 +1127,8 @@ cudaError_t launch_onesweep_passes(typename Tr::Bits* keys, typename Tr::Bits* t
     StatusT* cur = lb[p & 1];
     StatusT* next = (p + 1 < Tr::kPasses) ? lb[(p + 1) & 1] : nullptr;
     e = launch_kernel(rec, "radix_onesweep", kernel, dim3(unsigned(grid)), dim3(Shape::kBlock), sizeof(Smem), stream,
-                      keys, tmp, st, cur, next, n, uint32_t(L.num_tiles), p, use_tma ? 1 : 0, SegLarge{});
+                      keys, tmp, st, cur, next, n, uint32_t(L.num_tiles), p, use_tma ? 1 : 0, SegLarge{},
+                      static_cast<NoValue*>(nullptr), static_cast<NoValue*>(nullptr));
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
@@ -1063,13 +1158,39 @@ cudaError_t launch_onesweep_variant(typename Tr::Bits* keys, typename Tr::Bits* 
 #undef MGS_LAUNCH
 }
 
-template <class Tr>
-cudaError_t radix_sort_typed(typename Tr::Bits* keys, size_t n, void* temp, size_t temp_bytes, cudaStream_t stream,
-                             uint32_t* d_status, LaunchRecorder* rec) {
+// Key-value passes: one fixed tile shape per (key, value) width and ranking mode 3.
+template <class Tr, typename V, typename StatusT>
+cudaError_t launch_onesweep_pairs(typename Tr::Bits* keys, typename Tr::Bits* tmp, V* vals, V* vtmp, RadixState* st,
+                                  char* tbase, const RadixLayout& L, uint32_t n, bool use_tma, cudaStream_t stream,
+                                  LaunchRecorder* rec) {
+  using Shape = PairShape<int(sizeof(typename Tr::Bits)), int(sizeof(V))>;
+  using Smem = OnesweepSmem<Tr, Shape::kBlock, Shape::kItems, Shape::kChains, V>;
+  auto kernel = radix_onesweep_kernel<Tr, Shape::kBlock, Shape::kItems, Shape::kMinBlocks, Shape::kChains, StatusT,
+                                      3, false, V>;
+  static SmemLimitOnce attr;
+  cudaError_t e = attr.ensure(kernel, sizeof(Smem));
+  if (e != cudaSuccess) return e;
+  const size_t grid = std::min<size_t>(L.num_tiles, size_t(device_sm_count()));
+  StatusT* lb[2] = {reinterpret_cast<StatusT*>(tbase + L.lb0_off), reinterpret_cast<StatusT*>(tbase + L.lb1_off)};
+  for (int p = 0; p < Tr::kPasses; ++p) {
+    StatusT* cur = lb[p & 1];
+    StatusT* next = (p + 1 < Tr::kPasses) ? lb[(p + 1) & 1] : nullptr;
+    e = launch_kernel(rec, "radix_onesweep_pairs", kernel, dim3(unsigned(grid)), dim3(Shape::kBlock), sizeof(Smem),
+                      stream, keys, tmp, st, cur, next, n, uint32_t(L.num_tiles), p, use_tma ? 1 : 0, SegLarge{}, vals,
+                      vtmp);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+// Sorts keys (and, with a value type V, the values beside them) in place.
+template <class Tr, typename V = NoValue>
+cudaError_t radix_sort_impl(typename Tr::Bits* keys, V* vals, size_t n, void* temp, size_t temp_bytes,
+                            cudaStream_t stream, uint32_t* d_status, LaunchRecorder* rec) {
   using Bits = typename Tr::Bits;
   if (n == 0) return cudaSuccess;
   if (n >= (size_t(1) << 32)) return cudaErrorInvalidValue;
-  const RadixLayout L = radix_layout<Tr>(n);
+  const RadixLayout L = radix_layout<Tr, V>(n);
   if (temp == nullptr || temp_bytes < L.total) return cudaErrorInvalidValue;
   char* tb = static_cast<char*>(temp);
   RadixState* st = reinterpret_cast<RadixState*>(tb + L.state_off);
@@ -1093,17 +1214,39 @@ cudaError_t radix_sort_typed(typename Tr::Bits* keys, size_t n, void* temp, size
   e = launch_kernel(rec, "radix_scan", radix_scan_kernel, dim3(Tr::kPasses), dim3(kRadix), 0, stream, st, n32);
   if (e != cudaSuccess) return e;
 
-  const bool use_tma = (reinterpret_cast<uintptr_t>(keys) & 15u) == 0;
-  if (L.status_bytes == 4) {
-    e = launch_onesweep_variant<Tr, uint32_t>(keys, tmp, st, tb, L, n32, use_tma, stream, rec);
-  } else {
-    e = launch_onesweep_variant<Tr, unsigned long long>(keys, tmp, st, tb, L, n32, use_tma, stream, rec);
-  }
-  if (e != cudaSuccess) return e;
-
   const unsigned fin_grid = unsigned(std::max<size_t>(1, std::min<size_t>(size_t(sms) * 8, (n + 1023) / 1024)));
-  return launch_kernel(rec, "radix_finalize", radix_finalize_kernel<Tr>, dim3(fin_grid), dim3(256), 0, stream, keys,
-                       tmp, st, n32, d_status);
+  if constexpr (kHasValues<V>) {
+    V* vtmp = reinterpret_cast<V*>(tb + L.vals_off);
+    const bool use_tma = ((reinterpret_cast<uintptr_t>(keys) | reinterpret_cast<uintptr_t>(vals)) & 15u) == 0;
+    if (L.status_bytes == 4) {
+      e = launch_onesweep_pairs<Tr, V, uint32_t>(keys, tmp, vals, vtmp, st, tb, L, n32, use_tma, stream, rec);
+    } else {
+      e = launch_onesweep_pairs<Tr, V, unsigned long long>(keys, tmp, vals, vtmp, st, tb, L, n32, use_tma, stream,
+                                                           rec);
+    }
+    if (e != cudaSuccess) return e;
+    return launch_kernel(rec, "radix_finalize", radix_finalize_pairs_kernel<Tr, V>, dim3(fin_grid), dim3(256), 0,
+                         stream, keys, static_cast<const typename Tr::Bits*>(tmp), vals, static_cast<const V*>(vtmp),
+                         static_cast<const RadixState*>(st), n32, d_status);
+  } else {
+    (void)vals;
+    const bool use_tma = (reinterpret_cast<uintptr_t>(keys) & 15u) == 0;
+    if (L.status_bytes == 4) {
+      e = launch_onesweep_variant<Tr, uint32_t>(keys, tmp, st, tb, L, n32, use_tma, stream, rec);
+    } else {
+      e = launch_onesweep_variant<Tr, unsigned long long>(keys, tmp, st, tb, L, n32, use_tma, stream, rec);
+    }
+    if (e != cudaSuccess) return e;
+    return launch_kernel(rec, "radix_finalize", radix_finalize_kernel<Tr>, dim3(fin_grid), dim3(256), 0, stream, keys,
+                         tmp, st, n32, d_status);
+  }
+}
+
+template <class Tr>
+cudaError_t radix_sort_typed(typename Tr::Bits* keys, size_t n, void* temp, size_t temp_bytes, cudaStream_t stream,
+                             uint32_t* d_status, LaunchRecorder* rec) {
+  return radix_sort_impl<Tr, NoValue>(keys, static_cast<NoValue*>(nullptr), n, temp, temp_bytes, stream, d_status,
+                                      rec);
 }
 
 // ---------------------------------------------------------------- segmented host
@@ -1202,7 +1345,8 @@ cudaError_t segmented_sort_typed(typename Tr::Bits* keys, size_t n, const uint64
     for (int p = 0; p < Tr::kPasses; ++p) {
       uint32_t* next = (p + 1 < Tr::kPasses) ? lb[(p + 1) & 1] : nullptr;
       e = launch_kernel(rec, "seg_onesweep", kernel, dim3(unsigned(sms)), dim3(Shape::kBlock), sizeof(Smem), stream,
-                        keys, tmp, st, lb[p & 1], next, uint32_t(n), 0u, p, 1, sg);
+                        keys, tmp, st, lb[p & 1], next, uint32_t(n), 0u, p, 1, sg, static_cast<NoValue*>(nullptr),
+                        static_cast<NoValue*>(nullptr));
       if (e != cudaSuccess) return e;
     }
   }
@@ -1217,6 +1361,57 @@ size_t radix_sort_temp_bytes(int dtype, size_t n) {
   size_t bytes = 0;
   dispatch_dtype(dtype, [&](auto tr) { bytes = radix_layout<decltype(tr)>(n).total; });
   return bytes;
+}
+
+size_t radix_sort_pairs_temp_bytes(int dtype, size_t value_bytes, size_t n) {
+  size_t bytes = 0;
+  dispatch_dtype(dtype, [&](auto tr) {
+    using Tr = decltype(tr);
+    if (value_bytes == 4) bytes = radix_layout<Tr, uint32_t>(n).total;
+    if (value_bytes == 8) bytes = radix_layout<Tr, unsigned long long>(n).total;
+  });
+  return bytes;
+}
+
+cudaError_t radix_sort_pairs(int dtype, void* d_keys, void* d_values, size_t value_bytes, size_t n, void* d_temp,
+                             size_t temp_bytes, cudaStream_t stream, uint32_t* d_status, LaunchRecorder* rec) {
+  if (value_bytes != 4 && value_bytes != 8) return cudaErrorInvalidValue;
+  cudaError_t result = cudaErrorInvalidValue;
+  dispatch_dtype(dtype, [&](auto tr) {
+    using Tr = decltype(tr);
+    using Bits = typename Tr::Bits;
+    if (value_bytes == 4) {
+      result = radix_sort_impl<Tr, uint32_t>(static_cast<Bits*>(d_keys), static_cast<uint32_t*>(d_values), n, d_temp,
+                                             temp_bytes, stream, d_status, rec);
+    } else {
+      result = radix_sort_impl<Tr, unsigned long long>(static_cast<Bits*>(d_keys),
+                                                       static_cast<unsigned long long*>(d_values), n, d_temp,
+                                                       temp_bytes, stream, d_status, rec);
+    }
+  });
+  return result;
+}
+
+namespace {
+template <typename V>
+__global__ void iota_kernel(V* __restrict__ out, size_t n) {
+  const size_t stride = size_t(gridDim.x) * blockDim.x;
+  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) out[i] = V(i);
+}
+}  // namespace
+
+cudaError_t radix_argsort(int dtype, void* d_keys, void* d_indices, size_t index_bytes, size_t n, void* d_temp,
+                          size_t temp_bytes, cudaStream_t stream, uint32_t* d_status, LaunchRecorder* rec) {
+  if (index_bytes != 4 && index_bytes != 8) return cudaErrorInvalidValue;
+  if (n == 0) return cudaSuccess;
+  const unsigned grid = unsigned(std::max<size_t>(1, std::min<size_t>(size_t(device_sm_count()) * 8, (n + 255) / 256)));
+  cudaError_t e = index_bytes == 4
+                      ? launch_kernel(rec, "iota", iota_kernel<uint32_t>, dim3(grid), dim3(256), 0, stream,
+                                      static_cast<uint32_t*>(d_indices), n)
+                      : launch_kernel(rec, "iota", iota_kernel<unsigned long long>, dim3(grid), dim3(256), 0, stream,
+                                      static_cast<unsigned long long*>(d_indices), n);
+  if (e != cudaSuccess) return e;
+  return radix_sort_pairs(dtype, d_keys, d_indices, index_bytes, n, d_temp, temp_bytes, stream, d_status, rec);
 }
 
 int radix_sort_launches(int dtype, size_t n) {

@@ -34,6 +34,19 @@ cudaError_t segmented_sort(int dtype, void* d_keys, size_t n, const uint64_t* d_
                            void* d_temp, size_t temp_bytes, cudaStream_t stream, uint32_t* d_status,
                            LaunchRecorder* rec);
 
+// Key-value sort (thrust::sort_by_key order): d_keys[0..n) sorted as by
+// radix_sort, stably, and d_values[0..n) (value_bytes = 4 or 8, opaque) moved
+// with their keys. d_temp must hold radix_sort_pairs_temp_bytes() bytes.
+size_t radix_sort_pairs_temp_bytes(int dtype, size_t value_bytes, size_t n);
+cudaError_t radix_sort_pairs(int dtype, void* d_keys, void* d_values, size_t value_bytes, size_t n, void* d_temp,
+                             size_t temp_bytes, cudaStream_t stream, uint32_t* d_status, LaunchRecorder* rec);
+
+// Argsort: d_indices[0..n) (index_bytes = 4 or 8) receives the input position
+// of every key in sorted order; the keys are sorted in place on the way.
+// Scratch: radix_sort_pairs_temp_bytes(dtype, index_bytes, n).
+cudaError_t radix_argsort(int dtype, void* d_keys, void* d_indices, size_t index_bytes, size_t n, void* d_temp,
+                          size_t temp_bytes, cudaStream_t stream, uint32_t* d_status, LaunchRecorder* rec);
+
 // Number of kernel launches radix_sort issues for (dtype, n).
 int radix_sort_launches(int dtype, size_t n);
 

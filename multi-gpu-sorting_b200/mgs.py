@@ -101,6 +101,9 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "mgs_sort_temp_bytes": ([c_int, c_size, ctypes.POINTER(c_size)], c_int),
         "mgs_sort_device": ([c_void, c_int, c_void, c_size, c_void, c_size, c_void], c_int),
         "mgs_sort_host": ([c_void, c_int, c_void, c_size], c_int),
+        "mgs_sort_pairs_temp_bytes": ([c_int, c_size, c_size, ctypes.POINTER(c_size)], c_int),
+        "mgs_sort_pairs_device": ([c_void, c_int, c_void, c_void, c_size, c_size, c_void, c_size, c_void], c_int),
+        "mgs_argsort_device": ([c_void, c_int, c_void, c_void, c_size, c_size, c_void, c_size, c_void], c_int),
         "mgs_sort_device_noalloc": ([c_int, c_void, c_size, c_void], c_int),
         "mgs_generate": ([c_int, ctypes.c_char_p, c_u32, c_void, c_size], c_int),
         "mgs_tanasic_sort": ([c_void, c_int, c_void, c_size, c_int], c_int),
@@ -302,6 +305,28 @@ class Context:
         _check(self._lib.mgs_sort_device(self.handle, dtype_code(dtype), ctypes.c_void_p(d_keys), int(n),
                                          ctypes.c_void_p(d_temp or None), int(temp_bytes),
                                          ctypes.c_void_p(stream or None)))
+
+    # --- key-value sort and argsort (thrust::sort_by_key order) ---
+    @staticmethod
+    def sort_pairs_temp_bytes(dtype, value_bytes: int, n: int) -> int:
+        lib = load_library()
+        b = ctypes.c_size_t()
+        _check(lib.mgs_sort_pairs_temp_bytes(dtype_code(dtype), int(value_bytes), int(n), ctypes.byref(b)))
+        return b.value
+
+    def sort_pairs_device(self, d_keys: int, d_values: int, value_bytes: int, n: int, dtype, d_temp: int = 0,
+                          temp_bytes: int = 0, stream: int = 0) -> None:
+        _check(self._lib.mgs_sort_pairs_device(self.handle, dtype_code(dtype), ctypes.c_void_p(d_keys),
+                                               ctypes.c_void_p(d_values), int(value_bytes), int(n),
+                                               ctypes.c_void_p(d_temp or None), int(temp_bytes),
+                                               ctypes.c_void_p(stream or None)))
+
+    def argsort_device(self, d_keys: int, d_indices: int, index_bytes: int, n: int, dtype, d_temp: int = 0,
+                       temp_bytes: int = 0, stream: int = 0) -> None:
+        _check(self._lib.mgs_argsort_device(self.handle, dtype_code(dtype), ctypes.c_void_p(d_keys),
+                                            ctypes.c_void_p(d_indices), int(index_bytes), int(n),
+                                            ctypes.c_void_p(d_temp or None), int(temp_bytes),
+                                            ctypes.c_void_p(stream or None)))
 
     # --- TanasicSort with one GPU: host buffer in, sorted in place ---
     def sort_host(self, keys: np.ndarray) -> None:

@@ -278,6 +278,33 @@ int oracle_sort(int dtype, void* keys, size_t n) {
   });
 }
 
+// Key-value sort in the thrust::sort_by_key order (the reference's sort order,
+// stable: values of equal keys keep their input order). value_bytes is 4 or 8;
+// values are opaque payloads that follow their keys.
+int oracle_sort_pairs(int dtype, void* keys, void* values, size_t value_bytes, size_t n) {
+  if (value_bytes != 4 && value_bytes != 8) return 1;
+  return dispatch(dtype, [&](auto o) {
+    using P = Parts<decltype(o)>;
+    using U = typename P::Bits;
+    U* k = static_cast<U*>(keys);
+    std::vector<size_t> perm(n);
+    std::iota(perm.begin(), perm.end(), size_t(0));
+    std::stable_sort(perm.begin(), perm.end(),
+                     [&](size_t a, size_t b) { return Order<U, P::kKind>::less(k[a], k[b]); });
+    std::vector<U> kk(n);
+    std::vector<unsigned char> vv(n * value_bytes);
+    const unsigned char* v = static_cast<const unsigned char*>(values);
+    for (size_t i = 0; i < n; ++i) {
+      kk[i] = k[perm[i]];
+      std::memcpy(&vv[i * value_bytes], v + perm[i] * value_bytes, value_bytes);
+    }
+    if (n) {
+      std::memcpy(keys, kk.data(), n * sizeof(U));
+      std::memcpy(values, vv.data(), n * value_bytes);
+    }
+  });
+}
+
 // thrust::merge of two sorted ranges (src/tanasic_sort.cuh:163-167).
 int oracle_merge(int dtype, const void* a, size_t na, const void* b, size_t nb, void* out) {
   return dispatch(dtype, [&](auto o) {

@@ -39,6 +39,7 @@ def oracle_lib() -> ctypes.CDLL:
         lib.oracle_tanasic_sort.argtypes = [i, v, s, i]
         lib.oracle_kway_merge.argtypes = [i, ctypes.POINTER(v), ctypes.POINTER(s), i, v]
         lib.oracle_segmented_sort.argtypes = [i, v, ctypes.POINTER(ctypes.c_uint64), s]
+        lib.oracle_sort_pairs.argtypes = [i, v, v, s, s]
         lib.oracle_order_key.argtypes = [i, ctypes.c_uint64]
         lib.oracle_order_key.restype = ctypes.c_uint64
         _oracle = lib
@@ -64,6 +65,7 @@ def ref_lib() -> ctypes.CDLL:
         lib.ref_num_procs.restype = i
         lib.ref_cub_sort_device_ms.argtypes = [i, v, s, v, s, ctypes.POINTER(s)]
         lib.ref_cub_sort_device_ms.restype = ctypes.c_double
+        lib.ref_thrust_sort_by_key.argtypes = [i, v, v, s, s]
         _ref = lib
     return _ref
 
@@ -78,6 +80,16 @@ def sort(a: np.ndarray) -> np.ndarray:
     out = np.ascontiguousarray(a).copy()
     assert oracle_lib().oracle_sort(code(out), _ptr(out), out.size) == 0
     return out
+
+
+def sort_pairs(keys: np.ndarray, values: np.ndarray):
+    """thrust::sort_by_key order: keys sorted as by sort(), values following their keys, equal keys in input
+    order. Returns sorted copies (keys, values); values are 4- or 8-byte payloads."""
+    k = np.ascontiguousarray(keys).copy()
+    v = np.ascontiguousarray(values).copy()
+    assert k.size == v.size
+    assert oracle_lib().oracle_sort_pairs(code(k), _ptr(k), _ptr(v), v.dtype.itemsize, k.size) == 0
+    return k, v
 
 
 def merge(a: np.ndarray, b: np.ndarray) -> np.ndarray:
@@ -176,6 +188,12 @@ def ref_cub_sort_device_ms(dtype_code: int, d_keys: int, n: int, d_temp: int = 0
     ms = ref_lib().ref_cub_sort_device_ms(dtype_code, ctypes.c_void_p(d_keys), n, ctypes.c_void_p(d_temp or None),
                                           temp_bytes, ctypes.byref(need))
     return ms, need.value
+
+
+def ref_thrust_sort_by_key(dtype_code: int, d_keys: int, d_values: int, value_bytes: int, n: int) -> None:
+    """thrust::sort_by_key on device keys (of the given dtype code) and 4- or 8-byte values, in place."""
+    assert ref_lib().ref_thrust_sort_by_key(dtype_code, ctypes.c_void_p(d_keys), ctypes.c_void_p(d_values),
+                                            value_bytes, n) == 0
 
 
 def ref_num_procs() -> int:

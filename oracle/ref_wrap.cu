@@ -13,9 +13,14 @@
 //                          library call the reference times in
 //                          src/local_gpu_sort_algorithm_benchmark.cu:51-67 (CUDA events)
 //   ref_phase_seconds     TimeDurations phase                       src/time_durations.cuh
+//   ref_thrust_sort_by_key thrust::sort_by_key on device keys and 4- or 8-byte
+//                          values: the library the reference sorts with
+//                          (src/tanasic_sort.cuh:264), in its key-value form
 #include <omp.h>
 
 #include <cub/cub.cuh>
+#include <thrust/execution_policy.h>
+#include <thrust/sort.h>
 
 #include <cstdint>
 #include <cstring>
@@ -117,6 +122,24 @@ int ref_multiway_merge(int dtype, const void* const* runs, const size_t* lens, i
 // benchmark does (same pointer for input and output), and returns the CUDA-event time in ms of
 // the sort alone. d_temp must hold the bytes CUB asks for; temp_bytes 0 = query them (returned
 // through *need).
+int ref_thrust_sort_by_key(int dtype, void* d_keys, void* d_values, size_t value_bytes, size_t n) {
+  if (value_bytes != 4 && value_bytes != 8) return 1;
+  int rc = 0;
+  dispatch(dtype, [&](auto tag) {
+    using T = decltype(tag);
+    T* k = static_cast<T*>(d_keys);
+    if (value_bytes == 4) {
+      uint32_t* v = static_cast<uint32_t*>(d_values);
+      thrust::sort_by_key(thrust::device, k, k + n, v);
+    } else {
+      uint64_t* v = static_cast<uint64_t*>(d_values);
+      thrust::sort_by_key(thrust::device, k, k + n, v);
+    }
+    rc = cudaDeviceSynchronize() == cudaSuccess ? 0 : 2;
+  });
+  return rc;
+}
+
 double ref_cub_sort_device_ms(int dtype, void* d_keys, size_t n, void* d_temp, size_t temp_bytes, size_t* need) {
   double ms = -1.0;
   dispatch(dtype, [&](auto tag) {
