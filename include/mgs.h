@@ -190,6 +190,20 @@ int mgs_sort_pairs_device(mgs_ctx* ctx, int dtype, void* d_keys, void* d_values,
 int mgs_argsort_device(mgs_ctx* ctx, int dtype, void* d_keys, void* d_indices, size_t index_bytes, size_t n,
                        void* d_temp, size_t temp_bytes, void* stream);
 
+/* ---- bit ranges and descending order -----------------------------------------
+ * Not in the reference; the begin_bit / end_bit and descending forms of
+ * cub::DeviceRadixSort (SortKeys[Descending], SortPairs[Descending]), the
+ * library behind the thrust::sort the reference calls (src/tanasic_sort.cuh:264).
+ * Keys are compared by bits [begin_bit, end_bit) of their ordered form (the
+ * order of mgs_sort_device: unsigned, two's complement, IEEE with -0.0 equal to
+ * +0.0), ascending or descending (descending != 0); the sort is stable, so keys
+ * equal on those bits keep their input order. value_bytes 4 or 8 moves d_values
+ * with their keys; 0 sorts keys only (d_values unused). 0 <= begin_bit <=
+ * end_bit <= key bits. Scratch: mgs_sort_temp_bytes (keys only) or
+ * mgs_sort_pairs_temp_bytes; NULL: the context's arena. Asynchronous. */
+int mgs_sort_range_device(mgs_ctx* ctx, int dtype, void* d_keys, void* d_values, size_t value_bytes, size_t n,
+                          int begin_bit, int end_bit, int descending, void* d_temp, size_t temp_bytes, void* stream);
+
 /* ---- recorded sorts (CUDA graphs) -------------------------------------------
  * No counterpart in the reference (its sorts are host-driven thrust calls). A
  * plan records once, into a CUDA graph, the launches of one device sort or one

@@ -407,6 +407,42 @@ int mgs_argsort_device(mgs_ctx* ctx, int dtype, void* d_keys, void* d_indices, s
                     true);
 }
 
+int mgs_sort_range_device(mgs_ctx* ctx, int dtype, void* d_keys, void* d_values, size_t value_bytes, size_t n,
+                          int begin_bit, int end_bit, int descending, void* d_temp, size_t temp_bytes, void* stream) {
+  if (!ctx) return invalid("mgs_sort_range_device: ctx is null");
+  const size_t w = mgs::dtype_bytes(dtype);
+  if (w == 0) return invalid("mgs_sort_range_device: unknown dtype");
+  if (value_bytes != 0 && value_bytes != 4 && value_bytes != 8)
+    return invalid("mgs_sort_range_device: value_bytes must be 0, 4 or 8");
+  if (begin_bit < 0 || begin_bit > end_bit || end_bit > int(8 * w))
+    return invalid("mgs_sort_range_device: need 0 <= begin_bit <= end_bit <= key bits");
+  if (n == 0) return MGS_OK;
+  if (!d_keys || (value_bytes && !d_values)) return invalid("mgs_sort_range_device: null pointer");
+  if (reinterpret_cast<uintptr_t>(d_keys) % w != 0 ||
+      (value_bytes && reinterpret_cast<uintptr_t>(d_values) % value_bytes != 0))
+    return invalid("mgs_sort_range_device: keys or values are not aligned to their size");
+  if (n > kMaxDeviceSortKeys) return invalid("mgs_sort_range_device: n must be below 2^32");
+  Context& c = ctx->impl;
+  DeviceGuard g(c.device);
+  const size_t need =
+      value_bytes ? mgs::radix_sort_pairs_temp_bytes(dtype, value_bytes, n) : mgs::radix_sort_temp_bytes(dtype, n);
+  if (d_temp == nullptr) {
+    cudaError_t e = c.reserve(need);
+    if (e != cudaSuccess) return cuda_fail(e, "mgs_sort_range_device: arena");
+    d_temp = c.arena;
+    temp_bytes = c.arena_bytes;
+  } else if (temp_bytes < need) {
+    set_last_error("mgs_sort_range_device: d_temp holds %zu bytes, %zu needed", temp_bytes, need);
+    return MGS_ERR_INVALID;
+  }
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c.compute;
+  const cudaError_t e = mgs::radix_sort_range(dtype, d_keys, d_values, value_bytes, n, begin_bit, end_bit, descending,
+                                              d_temp, temp_bytes, s, c.d_status, &c.recorder);
+  if (e != cudaSuccess) return cuda_fail(e, "mgs_sort_range_device");
+  mgs::clear_last_error();
+  return MGS_OK;
+}
+
 int mgs_sort_host(mgs_ctx* ctx, int dtype, void* h_keys, size_t n) {
   if (!ctx) return invalid("mgs_sort_host: ctx is null");
   const size_t w = mgs::dtype_bytes(dtype);

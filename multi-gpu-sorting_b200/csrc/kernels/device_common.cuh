@@ -22,6 +22,7 @@ enum KeyKind : int { kUnsignedKey = 0, kSignedKey = 1, kFloatKey = 2 };
 template <typename BitsT, int KIND>
 struct KeyTraits {
   using Bits = BitsT;
+  static constexpr int kKind = KIND;
   static constexpr int kBits = int(sizeof(BitsT) * 8);
   static constexpr int kPasses = int(sizeof(BitsT));  // 8-bit digits
   static constexpr BitsT kSign = BitsT(1) << (kBits - 1);
@@ -38,6 +39,42 @@ struct KeyTraits {
   }
   // Strict "a before b" in radix order (equal keys are not before each other).
   __host__ __device__ __forceinline__ static bool Less(BitsT a, BitsT b) { return Ordered(a) < Ordered(b); }
+};
+
+// Digit extraction of the radix passes.
+//   PlainDigits: the 8-bit digits of the whole ordered key, ascending (the
+//                thrust::sort / CUB SortKeys order).
+//   RangeDigits: the 8-bit digits of bits [begin, end) of the ordered key (the
+//                last digit narrower when end - begin is not a multiple of 8),
+//                each reversed when descending (CUB's begin_bit / end_bit and
+//                SortKeysDescending). Passes beyond the range give every key
+//                digit 0, so the sort skips them as identities; the passes stay
+//                stable, so keys equal on the range keep their input order.
+//                Zeros of IEEE keys follow CUB's onesweep (every CUB sort of
+//                more than one tile of keys): ascending, both -0.0 and +0.0
+//                take the ordered pattern of +0.0; descending, both take that
+//                of -0.0. Over the whole key the two patterns are neighbours
+//                and the choice never shows; on a partial bit range it decides
+//                where zeros go.
+struct PlainDigits {
+  template <class Tr>
+  __device__ __forceinline__ uint32_t digit(typename Tr::Bits k, int pass) const {
+    return Tr::Digit(k, pass);
+  }
+};
+struct RangeDigits {
+  int begin, end, descending;
+  template <class Tr>
+  __device__ __forceinline__ uint32_t digit(typename Tr::Bits k, int pass) const {
+    const int shift = begin + 8 * pass;
+    const int width = min(max(end - shift, 0), 8);
+    if (width == 0) return 0u;  // shift < end <= key bits whenever width > 0
+    const uint32_t mask = (1u << width) - 1u;
+    typename Tr::Bits o = Tr::Ordered(k);
+    if (Tr::kKind == kFloatKey && descending && o == Tr::kSign) o = Tr::kSign - 1;  // zeros as -0.0
+    const uint32_t d = uint32_t(o >> shift) & mask;
+    return descending ? (mask ^ d) : d;
+  }
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {

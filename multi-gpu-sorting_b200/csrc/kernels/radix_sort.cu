@@ -132,10 +132,10 @@ __device__ __forceinline__ void unpack_v4<unsigned long long>(const uint4& q, un
 }
 
 // ---------------------------------------------------------------- K1 --------
-template <class Tr>
+template <class Tr, class Dg = PlainDigits>
 __global__ __launch_bounds__(kHistBlock, 1) void radix_histogram_kernel(const typename Tr::Bits* __restrict__ keys,
                                                                      uint32_t n, RadixState* __restrict__ st,
-                                                                     uint4* __restrict__ lb0, size_t lb0_vecs) {
+                                                                     uint4* __restrict__ lb0, size_t lb0_vecs, Dg dg) {
   using Bits = typename Tr::Bits;
   constexpr int P = Tr::kPasses;
   constexpr int C = HistCopies<Tr>::kCopies;
@@ -152,9 +152,8 @@ __global__ __launch_bounds__(kHistBlock, 1) void radix_histogram_kernel(const ty
 
   uint32_t* const copy = hist_smem + (threadIdx.x & (C - 1));
   auto count_key = [&](Bits k) {
-    const Bits o = Tr::Ordered(k);
 #pragma unroll
-    for (int p = 0; p < P; ++p) atomicAdd(copy + (p * kRadix + (uint32_t(o >> (8 * p)) & 0xFFu)) * C, 1u);
+    for (int p = 0; p < P; ++p) atomicAdd(copy + (p * kRadix + dg.template digit<Tr>(k, p)) * C, 1u);
   };
 
   const uintptr_t addr = reinterpret_cast<uintptr_t>(keys);
@@ -300,11 +299,11 @@ __device__ __forceinline__ uint32_t digit_peers(uint32_t d, bool ok, uint32_t* m
 // With values, src_val/dst_val are the value buffers of src/dst: every value
 // goes to the slot its key goes to.
 template <class Tr, int BLOCK, int ITEMS, int CHAINS, int MATCH, bool FULL, bool ALLOW_SKIP, typename V, class OnCounts,
-          class Between>
+          class Between, class Dg = PlainDigits>
 __device__ __forceinline__ bool rank_tile(OnesweepSmem<Tr, BLOCK, ITEMS, CHAINS, V>& sm, const typename Tr::Bits* src,
                                           typename Tr::Bits* dst, uint32_t valid, int pass, uint32_t* tile_count_out,
                                           OnCounts on_counts, Between between, const V* src_val = nullptr,
-                                          V* dst_val = nullptr) {
+                                          V* dst_val = nullptr, Dg dg = Dg{}) {
   using Bits = typename Tr::Bits;
   constexpr int kTile = BLOCK * ITEMS;
   constexpr int kChains = (BLOCK / 32) * CHAINS;
@@ -325,7 +324,7 @@ __device__ __forceinline__ bool rank_tile(OnesweepSmem<Tr, BLOCK, ITEMS, CHAINS,
     key[i] = src[idx];
     if constexpr (kHasValues<V>) val[i] = src_val[idx];
     uint32_t* cc = sm.ccount + (warp * CHAINS + i / kPerChain) * kRadix;
-    if (FULL || idx < valid) atomicAdd(&cc[Tr::Digit(key[i], pass)], 1u);
+    if (FULL || idx < valid) atomicAdd(&cc[dg.template digit<Tr>(key[i], pass)], 1u);
   }
   __syncthreads();
 
@@ -369,7 +368,7 @@ __device__ __forceinline__ bool rank_tile(OnesweepSmem<Tr, BLOCK, ITEMS, CHAINS,
       const int i = h * kPerChain + j;
       const uint32_t idx = wbase + i * 32 + lane;
       ok[h] = FULL || idx < valid;
-      d[h] = ok[h] ? Tr::Digit(key[i], pass) : (256u + lane);
+      d[h] = ok[h] ? dg.template digit<Tr>(key[i], pass) : (256u + lane);
       cc[h] = sm.ccount + (warp * CHAINS + h) * kRadix;
       mm[h] = sm.masks + (warp * CHAINS + h) * 2 * kRadix + (j & 1) * kRadix;
     }
@@ -433,11 +432,11 @@ struct ValueSpan {
 // the look-back as soon as they are known), look back over the segment's
 // earlier tiles while the other warps rank, scatter the digit runs (with their
 // values, svals being the tile's value buffer, when V is a value type).
-template <class Tr, int BLOCK, int ITEMS, int CHAINS, typename StatusT, int MATCH, bool FULL, typename V>
+template <class Tr, int BLOCK, int ITEMS, int CHAINS, typename StatusT, int MATCH, bool FULL, typename V, class Dg>
 __device__ __forceinline__ void onesweep_tile(OnesweepSmem<Tr, BLOCK, ITEMS, CHAINS, V>& sm, typename Tr::Bits* skeys,
                                               RadixState* __restrict__ st, StatusT* __restrict__ lb_cur,
                                               const TileSpan<Tr>& span, uint32_t tile, uint32_t valid, int pass,
-                                              V* svals, const ValueSpan<V>& vspan) {
+                                              V* svals, const ValueSpan<V>& vspan, Dg dg) {
   using Bits = typename Tr::Bits;
   using LW = LookbackWord<StatusT>;
   const int tid = threadIdx.x;
@@ -494,7 +493,7 @@ __device__ __forceinline__ void onesweep_tile(OnesweepSmem<Tr, BLOCK, ITEMS, CHA
         }
         sm.gbase[tid] = span.bucket[tid] + uint32_t(excl) - sm.tile_start[tid];
       },
-      svals, svals);
+      svals, svals, dg);
   __syncthreads();
 
   // Phase 3: consecutive threads write consecutive positions of one digit run.
@@ -504,7 +503,7 @@ __device__ __forceinline__ void onesweep_tile(OnesweepSmem<Tr, BLOCK, ITEMS, CHA
     const uint32_t idx = i * BLOCK + tid;
     if (FULL || idx < valid) {
       const Bits k = skeys[idx];
-      const uint32_t gpos = sm.gbase[Tr::Digit(k, pass)] + idx;
+      const uint32_t gpos = sm.gbase[dg.template digit<Tr>(k, pass)] + idx;
       if (gpos < span.seg_len) {
         span.dst[gpos] = k;
         if constexpr (kHasValues<V>) vspan.dst[gpos] = svals[idx];
@@ -544,13 +543,13 @@ __device__ __forceinline__ TileSpan<Tr> seg_span(const SegLarge& sg, const typen
 
 // vbuf0/vbuf1: the value buffers of buf0/buf1 (key-value sort), else null.
 template <class Tr, int BLOCK, int ITEMS, int MINB, int CHAINS, typename StatusT, int MATCH, bool SEG,
-          typename V = NoValue>
+          typename V = NoValue, class Dg = PlainDigits>
 __global__ __launch_bounds__(BLOCK, MINB) void radix_onesweep_kernel(typename Tr::Bits* buf0, typename Tr::Bits* buf1,
                                                                      RadixState* __restrict__ st,
                                                                      StatusT* __restrict__ lb_cur,
                                                                      StatusT* __restrict__ lb_next, uint32_t n,
                                                                      uint32_t num_tiles_arg, int pass, int use_tma,
-                                                                     SegLarge sg, V* vbuf0, V* vbuf1) {
+                                                                     SegLarge sg, V* vbuf0, V* vbuf1, Dg dg) {
   using Bits = typename Tr::Bits;
   using Smem = OnesweepSmem<Tr, BLOCK, ITEMS, CHAINS, V>;
   static_assert(!(SEG && kHasValues<V>), "the segmented sort carries no values");
@@ -655,10 +654,10 @@ __global__ __launch_bounds__(BLOCK, MINB) void radix_onesweep_kernel(typename Tr
     if constexpr (kHasValues<V>) svals = sm.vals.v[cur];
     if (valid == uint32_t(kTile)) {
       onesweep_tile<Tr, BLOCK, ITEMS, CHAINS, StatusT, MATCH, true>(sm, skeys, st, lb_cur, span, tile, valid, pass,
-                                                                    svals, vspan);
+                                                                    svals, vspan, dg);
     } else {
       onesweep_tile<Tr, BLOCK, ITEMS, CHAINS, StatusT, MATCH, false>(sm, skeys, st, lb_cur, span, tile, valid, pass,
-                                                                     svals, vspan);
+                                                                     svals, vspan, dg);
     }
     __syncthreads();
     cur ^= 1;
@@ -1065,12 +1064,14 @@ struct PairShape {
   static constexpr int kMinBlocks = 1, kChains = 1;
 };
 
-template <class Tr, typename V = NoValue>
+template <class Tr, typename V = NoValue, class Dg = PlainDigits>
 RadixLayout radix_layout(size_t n) {
   constexpr int w = int(sizeof(typename Tr::Bits));
   size_t tile;
   if constexpr (kHasValues<V>) {
     tile = size_t(PairShape<w, int(sizeof(V))>::kBlock) * PairShape<w, int(sizeof(V))>::kItems;
+  } else if constexpr (!std::is_same<Dg, PlainDigits>::value) {
+    tile = shape_tile<w, kDefaultShape>();  // range sorts run the default shape
   } else {
     constexpr size_t tiles[kNumShapes] = {shape_tile<w, 0>(), shape_tile<w, 1>(), shape_tile<w, 2>(),
                                            shape_tile<w, 3>(), shape_tile<w, 4>(), shape_tile<w, 5>(),
@@ -1102,14 +1103,14 @@ int device_sm_count() {
   return sms > 0 ? sms : 148;
 }
 
-template <class Tr, int SHAPE, typename StatusT, int MATCH>
+template <class Tr, int SHAPE, typename StatusT, int MATCH, class Dg = PlainDigits>
 cudaError_t launch_onesweep_passes(typename Tr::Bits* keys, typename Tr::Bits* tmp, RadixState* st, char* tbase,
                                    const RadixLayout& L, uint32_t n, bool use_tma, cudaStream_t stream,
-                                   LaunchRecorder* rec) {
+                                   LaunchRecorder* rec, Dg dg = Dg{}) {
   using Shape = OnesweepShape<sizeof(typename Tr::Bits), SHAPE>;
   using Smem = OnesweepSmem<Tr, Shape::kBlock, Shape::kItems, Shape::kChains>;
   auto kernel = radix_onesweep_kernel<Tr, Shape::kBlock, Shape::kItems, Shape::kMinBlocks, Shape::kChains, StatusT,
-                                      MATCH, false>;
+                                      MATCH, false, NoValue, Dg>;
   static SmemLimitOnce attr;
   cudaError_t e = attr.ensure(kernel, sizeof(Smem));
   if (e != cudaSuccess) return e;
@@ -1128,7 +1129,7 @@ cudaError_t launch_onesweep_passes(typename Tr::Bits* keys, typename Tr::Bits* t
     StatusT* next = (p + 1 < Tr::kPasses) ? lb[(p + 1) & 1] : nullptr;
     e = launch_kernel(rec, "radix_onesweep", kernel, dim3(unsigned(grid)), dim3(Shape::kBlock), sizeof(Smem), stream,
                       keys, tmp, st, cur, next, n, uint32_t(L.num_tiles), p, use_tma ? 1 : 0, SegLarge{},
-                      static_cast<NoValue*>(nullptr), static_cast<NoValue*>(nullptr));
+                      static_cast<NoValue*>(nullptr), static_cast<NoValue*>(nullptr), dg);
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
@@ -1159,14 +1160,14 @@ cudaError_t launch_onesweep_variant(typename Tr::Bits* keys, typename Tr::Bits* 
 }
 
 // Key-value passes: one fixed tile shape per (key, value) width and ranking mode 3.
-template <class Tr, typename V, typename StatusT>
+template <class Tr, typename V, typename StatusT, class Dg>
 cudaError_t launch_onesweep_pairs(typename Tr::Bits* keys, typename Tr::Bits* tmp, V* vals, V* vtmp, RadixState* st,
                                   char* tbase, const RadixLayout& L, uint32_t n, bool use_tma, cudaStream_t stream,
-                                  LaunchRecorder* rec) {
+                                  LaunchRecorder* rec, Dg dg) {
   using Shape = PairShape<int(sizeof(typename Tr::Bits)), int(sizeof(V))>;
   using Smem = OnesweepSmem<Tr, Shape::kBlock, Shape::kItems, Shape::kChains, V>;
   auto kernel = radix_onesweep_kernel<Tr, Shape::kBlock, Shape::kItems, Shape::kMinBlocks, Shape::kChains, StatusT,
-                                      3, false, V>;
+                                      3, false, V, Dg>;
   static SmemLimitOnce attr;
   cudaError_t e = attr.ensure(kernel, sizeof(Smem));
   if (e != cudaSuccess) return e;
@@ -1177,20 +1178,20 @@ cudaError_t launch_onesweep_pairs(typename Tr::Bits* keys, typename Tr::Bits* tm
     StatusT* next = (p + 1 < Tr::kPasses) ? lb[(p + 1) & 1] : nullptr;
     e = launch_kernel(rec, "radix_onesweep_pairs", kernel, dim3(unsigned(grid)), dim3(Shape::kBlock), sizeof(Smem),
                       stream, keys, tmp, st, cur, next, n, uint32_t(L.num_tiles), p, use_tma ? 1 : 0, SegLarge{}, vals,
-                      vtmp);
+                      vtmp, dg);
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
 }
 
 // Sorts keys (and, with a value type V, the values beside them) in place.
-template <class Tr, typename V = NoValue>
+template <class Tr, typename V = NoValue, class Dg = PlainDigits>
 cudaError_t radix_sort_impl(typename Tr::Bits* keys, V* vals, size_t n, void* temp, size_t temp_bytes,
-                            cudaStream_t stream, uint32_t* d_status, LaunchRecorder* rec) {
+                            cudaStream_t stream, uint32_t* d_status, LaunchRecorder* rec, Dg dg = Dg{}) {
   using Bits = typename Tr::Bits;
   if (n == 0) return cudaSuccess;
   if (n >= (size_t(1) << 32)) return cudaErrorInvalidValue;
-  const RadixLayout L = radix_layout<Tr, V>(n);
+  const RadixLayout L = radix_layout<Tr, V, Dg>(n);
   if (temp == nullptr || temp_bytes < L.total) return cudaErrorInvalidValue;
   char* tb = static_cast<char*>(temp);
   RadixState* st = reinterpret_cast<RadixState*>(tb + L.state_off);
@@ -1205,11 +1206,11 @@ cudaError_t radix_sort_impl(typename Tr::Bits* keys, V* vals, size_t n, void* te
   const unsigned hist_grid = unsigned(std::max<size_t>(1, std::min<size_t>(size_t(sms), want)));
   const size_t lb0_vecs = L.num_tiles * kRadix * L.status_bytes / 16;
   static SmemLimitOnce hist_attr;
-  e = hist_attr.ensure(radix_histogram_kernel<Tr>, HistCopies<Tr>::kSmemBytes);
+  e = hist_attr.ensure(radix_histogram_kernel<Tr, Dg>, HistCopies<Tr>::kSmemBytes);
   if (e != cudaSuccess) return e;
-  e = launch_kernel(rec, "radix_histogram", radix_histogram_kernel<Tr>, dim3(hist_grid), dim3(kHistBlock),
+  e = launch_kernel(rec, "radix_histogram", radix_histogram_kernel<Tr, Dg>, dim3(hist_grid), dim3(kHistBlock),
                     HistCopies<Tr>::kSmemBytes, stream, keys, n32, st, reinterpret_cast<uint4*>(tb + L.lb0_off),
-                    lb0_vecs);
+                    lb0_vecs, dg);
   if (e != cudaSuccess) return e;
   e = launch_kernel(rec, "radix_scan", radix_scan_kernel, dim3(Tr::kPasses), dim3(kRadix), 0, stream, st, n32);
   if (e != cudaSuccess) return e;
@@ -1219,10 +1220,10 @@ cudaError_t radix_sort_impl(typename Tr::Bits* keys, V* vals, size_t n, void* te
     V* vtmp = reinterpret_cast<V*>(tb + L.vals_off);
     const bool use_tma = ((reinterpret_cast<uintptr_t>(keys) | reinterpret_cast<uintptr_t>(vals)) & 15u) == 0;
     if (L.status_bytes == 4) {
-      e = launch_onesweep_pairs<Tr, V, uint32_t>(keys, tmp, vals, vtmp, st, tb, L, n32, use_tma, stream, rec);
+      e = launch_onesweep_pairs<Tr, V, uint32_t>(keys, tmp, vals, vtmp, st, tb, L, n32, use_tma, stream, rec, dg);
     } else {
       e = launch_onesweep_pairs<Tr, V, unsigned long long>(keys, tmp, vals, vtmp, st, tb, L, n32, use_tma, stream,
-                                                           rec);
+                                                           rec, dg);
     }
     if (e != cudaSuccess) return e;
     return launch_kernel(rec, "radix_finalize", radix_finalize_pairs_kernel<Tr, V>, dim3(fin_grid), dim3(256), 0,
@@ -1231,7 +1232,15 @@ cudaError_t radix_sort_impl(typename Tr::Bits* keys, V* vals, size_t n, void* te
   } else {
     (void)vals;
     const bool use_tma = (reinterpret_cast<uintptr_t>(keys) & 15u) == 0;
-    if (L.status_bytes == 4) {
+    if constexpr (!std::is_same<Dg, PlainDigits>::value) {
+      if (L.status_bytes == 4) {
+        e = launch_onesweep_passes<Tr, kDefaultShape, uint32_t, 3, Dg>(keys, tmp, st, tb, L, n32, use_tma, stream,
+                                                                       rec, dg);
+      } else {
+        e = launch_onesweep_passes<Tr, kDefaultShape, unsigned long long, 3, Dg>(keys, tmp, st, tb, L, n32, use_tma,
+                                                                                 stream, rec, dg);
+      }
+    } else if (L.status_bytes == 4) {
       e = launch_onesweep_variant<Tr, uint32_t>(keys, tmp, st, tb, L, n32, use_tma, stream, rec);
     } else {
       e = launch_onesweep_variant<Tr, unsigned long long>(keys, tmp, st, tb, L, n32, use_tma, stream, rec);
@@ -1346,7 +1355,7 @@ cudaError_t segmented_sort_typed(typename Tr::Bits* keys, size_t n, const uint64
       uint32_t* next = (p + 1 < Tr::kPasses) ? lb[(p + 1) & 1] : nullptr;
       e = launch_kernel(rec, "seg_onesweep", kernel, dim3(unsigned(sms)), dim3(Shape::kBlock), sizeof(Smem), stream,
                         keys, tmp, st, lb[p & 1], next, uint32_t(n), 0u, p, 1, sg, static_cast<NoValue*>(nullptr),
-                        static_cast<NoValue*>(nullptr));
+                        static_cast<NoValue*>(nullptr), PlainDigits{});
       if (e != cudaSuccess) return e;
     }
   }
@@ -1399,6 +1408,31 @@ __global__ void iota_kernel(V* __restrict__ out, size_t n) {
   for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) out[i] = V(i);
 }
 }  // namespace
+
+cudaError_t radix_sort_range(int dtype, void* d_keys, void* d_values, size_t value_bytes, size_t n, int begin_bit,
+                             int end_bit, int descending, void* d_temp, size_t temp_bytes, cudaStream_t stream,
+                             uint32_t* d_status, LaunchRecorder* rec) {
+  if (value_bytes != 0 && value_bytes != 4 && value_bytes != 8) return cudaErrorInvalidValue;
+  const RangeDigits dg{begin_bit, end_bit, descending ? 1 : 0};
+  cudaError_t result = cudaErrorInvalidValue;
+  dispatch_dtype(dtype, [&](auto tr) {
+    using Tr = decltype(tr);
+    using Bits = typename Tr::Bits;
+    if (begin_bit < 0 || end_bit > Tr::kBits || begin_bit > end_bit) return;
+    Bits* k = static_cast<Bits*>(d_keys);
+    if (value_bytes == 0) {
+      result = radix_sort_impl<Tr, NoValue, RangeDigits>(k, static_cast<NoValue*>(nullptr), n, d_temp, temp_bytes,
+                                                         stream, d_status, rec, dg);
+    } else if (value_bytes == 4) {
+      result = radix_sort_impl<Tr, uint32_t, RangeDigits>(k, static_cast<uint32_t*>(d_values), n, d_temp,
+                                                          temp_bytes, stream, d_status, rec, dg);
+    } else {
+      result = radix_sort_impl<Tr, unsigned long long, RangeDigits>(
+          k, static_cast<unsigned long long*>(d_values), n, d_temp, temp_bytes, stream, d_status, rec, dg);
+    }
+  });
+  return result;
+}
 
 cudaError_t radix_argsort(int dtype, void* d_keys, void* d_indices, size_t index_bytes, size_t n, void* d_temp,
                           size_t temp_bytes, cudaStream_t stream, uint32_t* d_status, LaunchRecorder* rec) {

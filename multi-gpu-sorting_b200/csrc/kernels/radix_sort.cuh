@@ -41,6 +41,14 @@ size_t radix_sort_pairs_temp_bytes(int dtype, size_t value_bytes, size_t n);
 cudaError_t radix_sort_pairs(int dtype, void* d_keys, void* d_values, size_t value_bytes, size_t n, void* d_temp,
                              size_t temp_bytes, cudaStream_t stream, uint32_t* d_status, LaunchRecorder* rec);
 
+// Sort by bits [begin_bit, end_bit) of the ordered key (CUB's begin_bit /
+// end_bit), ascending or descending, stable; with value_bytes 4 or 8 the values
+// move with their keys (0: keys only, d_values unused). Scratch as for
+// radix_sort (keys only) or radix_sort_pairs.
+cudaError_t radix_sort_range(int dtype, void* d_keys, void* d_values, size_t value_bytes, size_t n, int begin_bit,
+                             int end_bit, int descending, void* d_temp, size_t temp_bytes, cudaStream_t stream,
+                             uint32_t* d_status, LaunchRecorder* rec);
+
 // Argsort: d_indices[0..n) (index_bytes = 4 or 8) receives the input position
 // of every key in sorted order; the keys are sorted in place on the way.
 // Scratch: radix_sort_pairs_temp_bytes(dtype, index_bytes, n).

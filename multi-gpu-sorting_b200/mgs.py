@@ -104,6 +104,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "mgs_sort_pairs_temp_bytes": ([c_int, c_size, c_size, ctypes.POINTER(c_size)], c_int),
         "mgs_sort_pairs_device": ([c_void, c_int, c_void, c_void, c_size, c_size, c_void, c_size, c_void], c_int),
         "mgs_argsort_device": ([c_void, c_int, c_void, c_void, c_size, c_size, c_void, c_size, c_void], c_int),
+        "mgs_sort_range_device": ([c_void, c_int, c_void, c_void, c_size, c_size, c_int, c_int, c_int, c_void, c_size,
+                                   c_void], c_int),
         "mgs_sort_device_noalloc": ([c_int, c_void, c_size, c_void], c_int),
         "mgs_generate": ([c_int, ctypes.c_char_p, c_u32, c_void, c_size], c_int),
         "mgs_tanasic_sort": ([c_void, c_int, c_void, c_size, c_int], c_int),
@@ -327,6 +329,16 @@ class Context:
                                             ctypes.c_void_p(d_indices), int(index_bytes), int(n),
                                             ctypes.c_void_p(d_temp or None), int(temp_bytes),
                                             ctypes.c_void_p(stream or None)))
+
+    def sort_range_device(self, d_keys: int, n: int, dtype, begin_bit: int, end_bit: int, descending: bool = False,
+                          d_values: int = 0, value_bytes: int = 0, d_temp: int = 0, temp_bytes: int = 0,
+                          stream: int = 0) -> None:
+        """Sort by bits [begin_bit, end_bit) of the ordered keys, ascending or descending (mgs_sort_range_device)."""
+        _check(self._lib.mgs_sort_range_device(self.handle, dtype_code(dtype), ctypes.c_void_p(d_keys),
+                                               ctypes.c_void_p(d_values or None), int(value_bytes), int(n),
+                                               int(begin_bit), int(end_bit), 1 if descending else 0,
+                                               ctypes.c_void_p(d_temp or None), int(temp_bytes),
+                                               ctypes.c_void_p(stream or None)))
 
     # --- TanasicSort with one GPU: host buffer in, sorted in place ---
     def sort_host(self, keys: np.ndarray) -> None:

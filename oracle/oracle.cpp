@@ -305,6 +305,43 @@ int oracle_sort_pairs(int dtype, void* keys, void* values, size_t value_bytes, s
   });
 }
 
+// CUB's begin_bit / end_bit and descending forms (the library behind the
+// reference's thrust::sort): stable sort by bits [begin, end) of the ordered
+// key, reversed when descending; values (value_bytes 4 or 8, 0 = none) follow.
+int oracle_sort_range(int dtype, void* keys, void* values, size_t value_bytes, size_t n, int begin, int end,
+                      int descending) {
+  if (value_bytes != 0 && value_bytes != 4 && value_bytes != 8) return 1;
+  return dispatch(dtype, [&](auto o) {
+    using P = Parts<decltype(o)>;
+    using U = typename P::Bits;
+    U* k = static_cast<U*>(keys);
+    const int width = end - begin;
+    auto bits = [&](U x) -> U {
+      if (width <= 0) return U(0);
+      U full = Order<U, P::kKind>::key(x);
+      // CUB's onesweep maps both zeros of IEEE keys to the ordered pattern of -0.0 when descending
+      // (cub/block/radix_rank_sort_operations.cuh, BaseDigitExtractor), of +0.0 when ascending.
+      if (P::kKind == 2 && descending && full == Order<U, P::kKind>::kSign) full = Order<U, P::kKind>::kSign - 1;
+      const U ord = full >> begin;
+      return width >= int(sizeof(U) * 8) ? ord : U(ord & ((U(1) << width) - 1));
+    };
+    std::vector<size_t> perm(n);
+    std::iota(perm.begin(), perm.end(), size_t(0));
+    std::stable_sort(perm.begin(), perm.end(), [&](size_t a, size_t b) {
+      return descending ? bits(k[b]) < bits(k[a]) : bits(k[a]) < bits(k[b]);
+    });
+    std::vector<U> kk(n);
+    for (size_t i = 0; i < n; ++i) kk[i] = k[perm[i]];
+    if (n) std::memcpy(keys, kk.data(), n * sizeof(U));
+    if (value_bytes) {
+      std::vector<unsigned char> vv(n * value_bytes);
+      const unsigned char* v = static_cast<const unsigned char*>(values);
+      for (size_t i = 0; i < n; ++i) std::memcpy(&vv[i * value_bytes], v + perm[i] * value_bytes, value_bytes);
+      if (n) std::memcpy(values, vv.data(), n * value_bytes);
+    }
+  });
+}
+
 // thrust::merge of two sorted ranges (src/tanasic_sort.cuh:163-167).
 int oracle_merge(int dtype, const void* a, size_t na, const void* b, size_t nb, void* out) {
   return dispatch(dtype, [&](auto o) {

@@ -40,6 +40,7 @@ def oracle_lib() -> ctypes.CDLL:
         lib.oracle_kway_merge.argtypes = [i, ctypes.POINTER(v), ctypes.POINTER(s), i, v]
         lib.oracle_segmented_sort.argtypes = [i, v, ctypes.POINTER(ctypes.c_uint64), s]
         lib.oracle_sort_pairs.argtypes = [i, v, v, s, s]
+        lib.oracle_sort_range.argtypes = [i, v, v, s, s, i, i, i]
         lib.oracle_order_key.argtypes = [i, ctypes.c_uint64]
         lib.oracle_order_key.restype = ctypes.c_uint64
         _oracle = lib
@@ -66,6 +67,7 @@ def ref_lib() -> ctypes.CDLL:
         lib.ref_cub_sort_device_ms.argtypes = [i, v, s, v, s, ctypes.POINTER(s)]
         lib.ref_cub_sort_device_ms.restype = ctypes.c_double
         lib.ref_thrust_sort_by_key.argtypes = [i, v, v, s, s]
+        lib.ref_cub_sort_range.argtypes = [i, v, v, s, s, i, i, i]
         _ref = lib
     return _ref
 
@@ -90,6 +92,17 @@ def sort_pairs(keys: np.ndarray, values: np.ndarray):
     assert k.size == v.size
     assert oracle_lib().oracle_sort_pairs(code(k), _ptr(k), _ptr(v), v.dtype.itemsize, k.size) == 0
     return k, v
+
+
+def sort_range(keys: np.ndarray, begin_bit: int, end_bit: int, descending: bool = False, values=None):
+    """CUB begin_bit / end_bit (and descending) order: stable sort by bits [begin_bit, end_bit) of the ordered
+    keys. Returns sorted copies: keys, or (keys, values) when values are given."""
+    k = np.ascontiguousarray(keys).copy()
+    v = None if values is None else np.ascontiguousarray(values).copy()
+    vb = 0 if v is None else v.dtype.itemsize
+    assert oracle_lib().oracle_sort_range(code(k), _ptr(k), None if v is None else _ptr(v), vb, k.size, begin_bit,
+                                          end_bit, 1 if descending else 0) == 0
+    return k if v is None else (k, v)
 
 
 def merge(a: np.ndarray, b: np.ndarray) -> np.ndarray:
@@ -194,6 +207,13 @@ def ref_thrust_sort_by_key(dtype_code: int, d_keys: int, d_values: int, value_by
     """thrust::sort_by_key on device keys (of the given dtype code) and 4- or 8-byte values, in place."""
     assert ref_lib().ref_thrust_sort_by_key(dtype_code, ctypes.c_void_p(d_keys), ctypes.c_void_p(d_values),
                                             value_bytes, n) == 0
+
+
+def ref_cub_sort_range(dtype_code: int, d_keys: int, n: int, begin_bit: int, end_bit: int, descending: bool,
+                       d_values: int = 0, value_bytes: int = 0) -> None:
+    """cub::DeviceRadixSort::SortKeys/SortPairs[Descending] with begin_bit / end_bit, in place on device buffers."""
+    assert ref_lib().ref_cub_sort_range(dtype_code, ctypes.c_void_p(d_keys), ctypes.c_void_p(d_values or None),
+                                        value_bytes, n, begin_bit, end_bit, 1 if descending else 0) == 0
 
 
 def ref_num_procs() -> int:

@@ -13,6 +13,8 @@
 //                          library call the reference times in
 //                          src/local_gpu_sort_algorithm_benchmark.cu:51-67 (CUDA events)
 //   ref_phase_seconds     TimeDurations phase                       src/time_durations.cuh
+//   ref_cub_sort_range    cub::DeviceRadixSort with begin_bit / end_bit, ascending
+//                         or descending, keys or pairs
 //   ref_thrust_sort_by_key thrust::sort_by_key on device keys and 4- or 8-byte
 //                          values: the library the reference sorts with
 //                          (src/tanasic_sort.cuh:264), in its key-value form
@@ -122,6 +124,58 @@ int ref_multiway_merge(int dtype, const void* const* runs, const size_t* lens, i
 // benchmark does (same pointer for input and output), and returns the CUDA-event time in ms of
 // the sort alone. d_temp must hold the bytes CUB asks for; temp_bytes 0 = query them (returned
 // through *need).
+// cub::DeviceRadixSort::SortKeys[Descending] / SortPairs[Descending] with begin_bit / end_bit, in place
+// on device buffers (value_bytes 0 = keys only). Allocates its own output and scratch buffers.
+int ref_cub_sort_range(int dtype, void* d_keys, void* d_values, size_t value_bytes, size_t n, int begin_bit,
+                       int end_bit, int descending) {
+  if (value_bytes != 0 && value_bytes != 4 && value_bytes != 8) return 1;
+  int rc = 0;
+  dispatch(dtype, [&](auto tag) {
+    using T = decltype(tag);
+    T* k = static_cast<T*>(d_keys);
+    T* k_out = nullptr;
+    void* v_out = nullptr;
+    void* temp = nullptr;
+    size_t bytes = 0;
+    if (cudaMalloc(&k_out, n * sizeof(T) + 16) != cudaSuccess) {
+      rc = 2;
+      return;
+    }
+    if (value_bytes) cudaMalloc(&v_out, n * value_bytes + 16);
+    auto run = [&](auto* v_in, auto* v_o) {
+      for (int pass = 0; pass < 2; ++pass) {  // size query, then the sort
+        if (value_bytes == 0) {
+          if (descending)
+            cub::DeviceRadixSort::SortKeysDescending(temp, bytes, k, k_out, n, begin_bit, end_bit);
+          else
+            cub::DeviceRadixSort::SortKeys(temp, bytes, k, k_out, n, begin_bit, end_bit);
+        } else {
+          if (descending)
+            cub::DeviceRadixSort::SortPairsDescending(temp, bytes, k, k_out, v_in, v_o, n, begin_bit, end_bit);
+          else
+            cub::DeviceRadixSort::SortPairs(temp, bytes, k, k_out, v_in, v_o, n, begin_bit, end_bit);
+        }
+        if (pass == 0 && cudaMalloc(&temp, bytes + 16) != cudaSuccess) {
+          rc = 3;
+          return;
+        }
+      }
+    };
+    if (value_bytes == 8) {
+      run(static_cast<uint64_t*>(d_values), static_cast<uint64_t*>(v_out));
+    } else {
+      run(static_cast<uint32_t*>(d_values), static_cast<uint32_t*>(v_out));
+    }
+    if (rc == 0 && cudaDeviceSynchronize() != cudaSuccess) rc = 4;
+    if (rc == 0) cudaMemcpy(d_keys, k_out, n * sizeof(T), cudaMemcpyDeviceToDevice);
+    if (rc == 0 && value_bytes) cudaMemcpy(d_values, v_out, n * value_bytes, cudaMemcpyDeviceToDevice);
+    cudaFree(k_out);
+    if (v_out) cudaFree(v_out);
+    if (temp) cudaFree(temp);
+  });
+  return rc;
+}
+
 int ref_thrust_sort_by_key(int dtype, void* d_keys, void* d_values, size_t value_bytes, size_t n) {
   if (value_bytes != 4 && value_bytes != 8) return 1;
   int rc = 0;
