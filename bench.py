@@ -532,7 +532,7 @@ def sweep_merge(mgs, torch, n, reps=3):
     ctx.close()
 
 
-def sweep_pairs(mgs, torch, reps=3):
+def sweep_pairs(mgs, torch, n32=1 << 30, reps=3):
     """Key-value sort (thrust::sort_by_key order) on device-resident data: 2^30 u32 keys with u32 values and 2^29
     u64 keys with u64 values; the values are the input positions, so the result is checked by gathering the input
     through them (ascending, a permutation, equal keys in input order). Algorithmic bytes: every pass reads and
@@ -540,7 +540,7 @@ def sweep_pairs(mgs, torch, reps=3):
     ctx = mgs.Context(0)
     peak, _ = measured_hbm_peak()
     stream = torch.cuda.Stream()
-    for dtype, n, vb in (("u32", 1 << 30, 4), ("u64", 1 << 29, 8)):
+    for dtype, n, vb in (("u32", n32, 4), ("u64", n32 // 2, 8)):
         w = 4 if dtype == "u32" else 8
         st = torch.int32 if w == 4 else torch.int64
         vt = torch.int32 if vb == 4 else torch.int64
@@ -738,7 +738,7 @@ def main():
         if args.sweep == "types":
             sweep_types(mgs, torch, args.sweep_n or N_KEYS)
         elif args.sweep == "pairs":
-            sweep_pairs(mgs, torch)
+            sweep_pairs(mgs, torch, args.sweep_n or (1 << 30))
         elif args.sweep == "tune":
             sweep_tune(mgs, args.tune_out, args.sweep_n or (1 << 28))
         elif args.sweep == "merge":
