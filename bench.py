@@ -126,6 +126,21 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def max_over_ranks(dist, world: int, value: float, device) -> float:
+    """The job's time: the slowest rank's value (all-reduce MAX); with one rank, the value itself."""
+    if world <= 1:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_keys_per_s(world: int, keys_per_rank: int, steps: int, seconds: float) -> float:
+    """Whole-job throughput: every rank's keys over the slowest rank's time (weak scaling)."""
+    return world * keys_per_rank * steps / seconds
+
+
 def zipf_segment_offsets(rng, nseg=100_000, total=1 << 28, s=1.2, max_len=1 << 22):
     """Batched workload: nseg segments with Zipf(s) lengths in [1, max_len], rescaled to about `total`
     keys (floor, at least 1 key), in random order."""
@@ -802,12 +817,8 @@ def main():
     ctx.set_profiling(False)
     ctx.synchronize()
     step_ms = [a.elapsed_time(b) for a, b in evs]
-    total_ms = sum(step_ms)
-    if world > 1:
-        t = torch.tensor([total_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = world * n * args.steps / (total_ms / 1e3)
+    total_ms = max_over_ranks(dist, world, sum(step_ms), "cuda")
+    value = job_keys_per_s(world, n, args.steps, total_ms / 1e3)
 
     # end to end through the public host API (mgs_sort_host), pinned buffers
     h = mgs.host_empty(n, np.uint32)
@@ -822,12 +833,8 @@ def main():
         if i > 0:  # first call warms the arena
             e2e_times.append(dt)
     e2e_ok = bool(np.all(h[1:] >= h[:-1]))
-    e2e_s = sum(e2e_times)
-    if world > 1:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_value = world * n * len(e2e_times) / e2e_s if e2e_times else None
+    e2e_s = max_over_ranks(dist, world, sum(e2e_times), "cuda")
+    e2e_value = job_keys_per_s(world, n, len(e2e_times), e2e_s) if e2e_times else None
 
     peak, peak_kind = measured_hbm_peak()
     one = ktimes.get("radix_onesweep", (0, 0.0))
