@@ -25,6 +25,8 @@
 #include <thrust/sort.h>
 
 #include <cstdint>
+#include <cstdio>
+#include <exception>
 #include <cstring>
 #include <parallel/algorithm>
 #include <string>
@@ -52,6 +54,28 @@ int dispatch(int dtype, Fn&& fn) {
   }
 }
 
+// Runs one wrapper body: clears the runtime's last error first (the reference
+// ignores CUDA errors in release builds, src/cuda_error.cuh:5-10, so a failed
+// call inside it can leave a non-sticky error that thrust would later report as
+// its own), turns C++ exceptions (thrust::system_error, std::bad_alloc) into a
+// return code with the message on stderr instead of terminating the process,
+// and clears what the body itself left behind.
+template <typename R, typename F>
+R guarded(R on_error, F&& body) {
+  cudaGetLastError();
+  try {
+    R r = body();
+    cudaGetLastError();
+    return r;
+  } catch (const std::exception& e) {
+    std::fprintf(stderr, "libref: %s\n", e.what());
+  } catch (...) {
+    std::fprintf(stderr, "libref: unknown exception\n");
+  }
+  cudaGetLastError();
+  return on_error;
+}
+
 }  // namespace
 
 extern "C" {
@@ -69,26 +93,26 @@ int ref_generate(int dtype, const char* distribution, uint32_t seed, void* out, 
 }
 
 int ref_tanasic_sort(int dtype, void* keys, size_t n, int device) {
-  return dispatch(dtype, [&](auto tag) {
+  return guarded(9, [&] { return dispatch(dtype, [&](auto tag) {
     using T = decltype(tag);
     std::vector<int> gpus{device};
     HostVector<T> elements(static_cast<T*>(keys), static_cast<T*>(keys) + n);
     SetupTanasicSort(gpus);
     TanasicSort<T>(&elements, gpus);
     if (n > 0) std::memcpy(keys, thrust::raw_pointer_cast(elements.data()), n * sizeof(T));
-  });
+  }); });
 }
 
 int ref_gowanlock_sort(int dtype, void* keys, size_t n, size_t chunk_size, size_t merge_group_size,
                        size_t num_buffers, int device, int num_threads) {
-  return dispatch(dtype, [&](auto tag) {
+  return guarded(9, [&] { return dispatch(dtype, [&](auto tag) {
     using T = decltype(tag);
     std::vector<int> gpus{device};
     HostVector<T> elements(static_cast<T*>(keys), static_cast<T*>(keys) + n);
     SetupGowanlockSort(gpus, num_threads);
     GowanlockSort<T>(&elements, chunk_size, merge_group_size, num_buffers, gpus);
     if (n > 0) std::memcpy(keys, thrust::raw_pointer_cast(elements.data()), n * sizeof(T));
-  });
+  }); });
 }
 
 int ref_gnu_parallel_sort(int dtype, void* keys, size_t n, int num_threads) {
@@ -129,6 +153,7 @@ int ref_multiway_merge(int dtype, const void* const* runs, const size_t* lens, i
 int ref_cub_sort_range(int dtype, void* d_keys, void* d_values, size_t value_bytes, size_t n, int begin_bit,
                        int end_bit, int descending) {
   if (value_bytes != 0 && value_bytes != 4 && value_bytes != 8) return 1;
+  return guarded(9, [&] {
   int rc = 0;
   dispatch(dtype, [&](auto tag) {
     using T = decltype(tag);
@@ -174,10 +199,12 @@ int ref_cub_sort_range(int dtype, void* d_keys, void* d_values, size_t value_byt
     if (temp) cudaFree(temp);
   });
   return rc;
+  });
 }
 
 int ref_thrust_sort_by_key(int dtype, void* d_keys, void* d_values, size_t value_bytes, size_t n) {
   if (value_bytes != 4 && value_bytes != 8) return 1;
+  return guarded(9, [&] {
   int rc = 0;
   dispatch(dtype, [&](auto tag) {
     using T = decltype(tag);
@@ -192,9 +219,11 @@ int ref_thrust_sort_by_key(int dtype, void* d_keys, void* d_values, size_t value
     rc = cudaDeviceSynchronize() == cudaSuccess ? 0 : 2;
   });
   return rc;
+  });
 }
 
 double ref_cub_sort_device_ms(int dtype, void* d_keys, size_t n, void* d_temp, size_t temp_bytes, size_t* need) {
+  return guarded(-2.0, [&] {
   double ms = -1.0;
   dispatch(dtype, [&](auto tag) {
     using T = decltype(tag);
@@ -217,6 +246,7 @@ double ref_cub_sort_device_ms(int dtype, void* d_keys, size_t n, void* d_temp, s
     cudaEventDestroy(b);
   });
   return ms;
+  });
 }
 
 double ref_phase_seconds(const char* phase) { return TimeDurations::Get()->durations[phase].count(); }
