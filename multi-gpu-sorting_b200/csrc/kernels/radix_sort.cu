@@ -239,44 +239,35 @@ struct OnesweepSmem {
   alignas(16) unsigned char span[2][48];  // TileSpan of the current / prefetched tile
 };
 
-// Peer mask of lanes holding the same digit (the warp multisplit step).
-//   MATCH 0: match.any (one instruction, but it issues many XU-pipe operations)
-//   MATCH 1: 8 ballots, one per digit bit (integer-ALU work)
+// Peer mask of lanes holding the same digit (the warp multisplit step), two
+// measured ways:
 //   MATCH 2: per-chain shared-memory masks: every lane ORs its bit into the
 //            mask of its digit, reads the mask back, and the last lane of each
 //            group clears it (masks alternate between two arrays per item).
-//   MATCH 3: ballots for half of the items (alternate items, or chain 0 of two),
-//            shared-memory masks for the rest, so that the integer-ALU work of
-//            one item overlaps the shared-memory latency of the next.
-//   MATCH 4: ballots for every fourth item, shared-memory masks otherwise.
+//   MATCH 3: ballots (8, one per digit bit) for half of the items (alternate
+//            items, or chain 0 of two), shared-memory masks for the rest, so
+//            that the integer-ALU work of one item overlaps the shared-memory
+//            latency of the next.
 // `ok` separates padding lanes of a partial tile (their digit is 256 + lane).
 template <int MATCH, int CHAINS>
 __device__ __forceinline__ constexpr bool rank_by_ballot(int h, int j) {
-  return MATCH == 1 || (MATCH == 3 && (CHAINS == 1 ? (j & 1) == 0 : h == 0)) || (MATCH == 4 && (j & 3) == 0);
+  return MATCH == 3 && (CHAINS == 1 ? (j & 1) == 0 : h == 0);
 }
 
-template <int MATCH, bool FULL>
-__device__ __forceinline__ uint32_t digit_peers(uint32_t d, bool ok, uint32_t* mm, int lane) {
-  if (MATCH == 0) {
-    return __match_any_sync(0xffffffffu, d);
-  } else if (MATCH == 1) {
-    uint32_t peers = 0xffffffffu;
+template <bool FULL>
+__device__ __forceinline__ uint32_t ballot_peers(uint32_t d, bool ok) {
+  uint32_t peers = 0xffffffffu;
 #pragma unroll
-    for (int b = 0; b < 8; ++b) {
-      const bool bit = (d >> b) & 1u;
-      const uint32_t bal = __ballot_sync(0xffffffffu, bit);
-      peers &= bit ? bal : ~bal;
-    }
-    if (!FULL) {
-      const uint32_t bal = __ballot_sync(0xffffffffu, ok);
-      peers &= ok ? bal : ~bal;
-    }
-    return peers;
-  } else {
-    if (ok) atomicOr(&mm[d], 1u << lane);
-    __syncwarp();
-    return ok ? mm[d] : (1u << lane);
+  for (int b = 0; b < 8; ++b) {
+    const bool bit = (d >> b) & 1u;
+    const uint32_t bal = __ballot_sync(0xffffffffu, bit);
+    peers &= bit ? bal : ~bal;
   }
+  if (!FULL) {
+    const uint32_t bal = __ballot_sync(0xffffffffu, ok);
+    peers &= ok ? bal : ~bal;
+  }
+  return peers;
 }
 
 // Phases 1-2 of ranking a tile held in shared memory: stable rank of `valid`
@@ -309,6 +300,7 @@ __device__ __forceinline__ bool rank_tile(OnesweepSmem<Tr, BLOCK, ITEMS, CHAINS,
   constexpr int kChains = (BLOCK / 32) * CHAINS;
   constexpr int kPerChain = ITEMS / CHAINS;
   static_assert(ITEMS % CHAINS == 0, "items split evenly into chains");
+  static_assert(MATCH == 2 || MATCH == 3, "ranking modes: shared-memory masks, or half ballots");
   const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
   const int wbase = warp * 32 * ITEMS;
@@ -372,19 +364,14 @@ __device__ __forceinline__ bool rank_tile(OnesweepSmem<Tr, BLOCK, ITEMS, CHAINS,
       cc[h] = sm.ccount + (warp * CHAINS + h) * kRadix;
       mm[h] = sm.masks + (warp * CHAINS + h) * 2 * kRadix + (j & 1) * kRadix;
     }
-    if (MATCH >= 2) {
 #pragma unroll
-      for (int h = 0; h < CHAINS; ++h)
-        if (!rank_by_ballot<MATCH, CHAINS>(h, j) && ok[h]) atomicOr(&mm[h][d[h]], 1u << lane);
-      __syncwarp();
+    for (int h = 0; h < CHAINS; ++h)
+      if (!rank_by_ballot<MATCH, CHAINS>(h, j) && ok[h]) atomicOr(&mm[h][d[h]], 1u << lane);
+    __syncwarp();
 #pragma unroll
-      for (int h = 0; h < CHAINS; ++h)
-        peers[h] = rank_by_ballot<MATCH, CHAINS>(h, j) ? digit_peers<1, FULL>(d[h], ok[h], mm[h], lane)
-                                                         : (ok[h] ? mm[h][d[h]] : (1u << lane));
-    } else {
-#pragma unroll
-      for (int h = 0; h < CHAINS; ++h) peers[h] = digit_peers<MATCH, FULL>(d[h], ok[h], mm[h], lane);
-    }
+    for (int h = 0; h < CHAINS; ++h)
+      peers[h] = rank_by_ballot<MATCH, CHAINS>(h, j) ? ballot_peers<FULL>(d[h], ok[h])
+                                                       : (ok[h] ? mm[h][d[h]] : (1u << lane));
 #pragma unroll
     for (int h = 0; h < CHAINS; ++h) pos[h] = ok[h] ? cc[h][d[h]] + __popc(peers[h] & lmask) : 0u;
     __syncwarp();
@@ -392,12 +379,11 @@ __device__ __forceinline__ bool rank_tile(OnesweepSmem<Tr, BLOCK, ITEMS, CHAINS,
     for (int h = 0; h < CHAINS; ++h) {
       if (ok[h] && (peers[h] & lmask_gt) == 0) {
         cc[h][d[h]] = pos[h] + 1u;  // the last lane of each peer group advances the counter
-        if (MATCH >= 2 && !rank_by_ballot<MATCH, CHAINS>(h, j)) mm[h][d[h]] = 0u;
+        if (!rank_by_ballot<MATCH, CHAINS>(h, j)) mm[h][d[h]] = 0u;
       }
     }
-    // With shared-memory masks the next item's first __syncwarp orders these
-    // counter updates before its counter reads; ballots and match need one here.
-    if (MATCH < 2) __syncwarp();
+    // The next item's first __syncwarp orders these counter updates (and mask
+    // clears) before its counter reads.
 #pragma unroll
     for (int h = 0; h < CHAINS; ++h) {
       if (ok[h] && pos[h] < uint32_t(kTile)) {
@@ -602,8 +588,7 @@ __global__ __launch_bounds__(BLOCK, MINB) void radix_onesweep_kernel(typename Tr
   // processed and the look-back makes progress.
   static_assert(sizeof(TileSpan<Tr>) <= sizeof(sm.span[0]), "span slot");
   TileSpan<Tr>* spans = reinterpret_cast<TileSpan<Tr>*>(sm.span);
-  if (MATCH >= 2)
-    for (int i = tid; i < kChains * 2 * kRadix; i += BLOCK) sm.masks[i] = 0u;
+  for (int i = tid; i < kChains * 2 * kRadix; i += BLOCK) sm.masks[i] = 0u;
   if (tid == 0) {
     mbar_init(&sm.bar[0], 1);
     mbar_init(&sm.bar[1], 1);
