@@ -422,8 +422,11 @@ def sweep_types(mgs, torch, n, reps=3):
         temp = torch.empty(temp_bytes, dtype=torch.uint8, device="cuda")
         for dist in SWEEP_DISTS:
             name = dist + ("-specials" if dtype == "f32" else "")
-            keys = mgs.generate(dtype, name, SEED, n)
-            src = torch.from_numpy(keys.view(storage[0])).cuda()
+            src = torch.empty(n, dtype=storage[1], device="cuda")
+            if dist == "normal0":  # log / cos of the host C library: generated on the host
+                src.copy_(torch.from_numpy(mgs.generate(dtype, name, SEED, n).view(storage[0])))
+            else:  # the same bytes, generated in place on the device
+                ctx.generate_device(src.data_ptr(), n, dtype, name, SEED)
             work = torch.empty_like(src)
             times = []
             for i in range(reps + 1):
@@ -445,6 +448,33 @@ def sweep_types(mgs, torch, n, reps=3):
                   flush=True)
             del src, work
         del temp
+    ctx.close()
+
+
+def sweep_generate(mgs, torch, n):
+    """Input generation of n keys on the device (mgs_generate_device) against the host generator (mgs_generate,
+    all host threads) producing the same bytes: wall-clock seconds of each call and whether the bytes agree."""
+    ctx = mgs.Context(0)
+    cases = [("u32", "uniform"), ("u32", "full-uniform"), ("u32", "zipf"), ("u32", "sorted"), ("u32", "staggered"),
+             ("f32", "nearly-sorted-swaps-specials"), ("u64", "full-uniform"), ("f64", "bucket-sorted")]
+    for dtype, dist in cases:
+        dt = mgs.np_dtype(dtype)
+        st_np, st_t = (np.int32, torch.int32) if dt.itemsize == 4 else (np.int64, torch.int64)
+        d = torch.empty(n, dtype=st_t, device="cuda")
+        ctx.generate_device(d.data_ptr(), min(n, 1 << 20), dtype, dist, SEED)  # loads the kernels
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ctx.generate_device(d.data_ptr(), n, dtype, dist, SEED)
+        dev_s = time.perf_counter() - t0
+        h = mgs.host_empty(n, dt)
+        t0 = time.perf_counter()
+        mgs.generate(dtype, dist, SEED, n, out=h)
+        host_s = time.perf_counter() - t0
+        same = bool(torch.equal(d, torch.from_numpy(h.view(st_np)).cuda()))
+        print(json.dumps({"sweep": "generate", "dtype": dtype, "distribution": dist, "n": n, "device_s": dev_s,
+                          "host_s": host_s, "host_threads": os.cpu_count(), "speedup": host_s / dev_s,
+                          "bytes_identical": same}), flush=True)
+        del d, h
     ctx.close()
 
 
@@ -732,7 +762,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched (segmented) measurement")
     ap.add_argument("--no-served", action="store_true", help="skip the serving-loop measurement")
-    ap.add_argument("--sweep", choices=["types", "merge", "ooc", "tune", "pairs"],
+    ap.add_argument("--sweep", choices=["types", "merge", "ooc", "tune", "pairs", "generate"],
                     help="measure another workload of the sort API instead (one JSON line per case)")
     ap.add_argument("--sweep-n", type=int, default=0, help="keys per case of --sweep (0: the workload's default)")
     ap.add_argument("--tune-out", default="", help="--sweep tune: write the tuned variant table to this file")
@@ -752,6 +782,8 @@ def main():
         mgs = load_mgs()
         if args.sweep == "types":
             sweep_types(mgs, torch, args.sweep_n or N_KEYS)
+        elif args.sweep == "generate":
+            sweep_generate(mgs, torch, args.sweep_n or N_KEYS)
         elif args.sweep == "pairs":
             sweep_pairs(mgs, torch, args.sweep_n or (1 << 30))
         elif args.sweep == "tune":

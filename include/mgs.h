@@ -332,6 +332,18 @@ int mgs_server_stats_get(mgs_server* server, mgs_server_stats* out, int reset);
  * of the keys with -0.0 and 0.1% with NaNs of both signs. */
 int mgs_generate(int dtype, const char* distribution, uint32_t seed, void* out, size_t n);
 
+/* ---- DataGenerator::ComputeDistribution<T> into device memory
+ * (src/data_generator.cuh:18-36, with the buffer on the GPU) ----
+ * Fills the device buffer d_out[0..n) with the same bytes mgs_generate writes
+ * for the same (dtype, distribution, seed, n), without the host generation and
+ * the copy. Every distribution above except "normal", "nearly-sorted" and
+ * "normal0": those draw through the host C library's log / cos, which the
+ * device does not reproduce bit for bit, and are refused (MGS_ERR_INVALID).
+ * Entries the host generator leaves untouched (staggered and bucket-sorted with
+ * n < 10) stay untouched. Uses the context's arena and compute stream; returns
+ * when the buffer is filled. n must be below 2^32. */
+int mgs_generate_device(mgs_ctx* ctx, int dtype, const char* distribution, uint32_t seed, void* d_out, size_t n);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

@@ -19,9 +19,8 @@
 #include "context.h"
 #include "out_of_core.h"
 
-namespace mgs {
-bool generate_keys(int dtype, const char* distribution, uint32_t seed, void* out, size_t n);
-}
+#include "data_generator.h"
+#include "../kernels/generate.cuh"
 
 using mgs::Context;
 using mgs::set_last_error;
@@ -838,6 +837,32 @@ int mgs_generate(int dtype, const char* distribution, uint32_t seed, void* out, 
   }
   mgs::clear_last_error();
   return MGS_OK;
+}
+
+int mgs_generate_device(mgs_ctx* ctx, int dtype, const char* distribution, uint32_t seed, void* d_out, size_t n) {
+  if (!ctx) return invalid("mgs_generate_device: ctx is null");
+  if (!distribution) return invalid("mgs_generate_device: distribution is null");
+  size_t need = 0;
+  std::string why;
+  if (!mgs::generate_device_temp_bytes(dtype, distribution, n, &need, &why)) {
+    set_last_error("mgs_generate_device: %s", why.c_str());
+    return MGS_ERR_INVALID;
+  }
+  if (n == 0) return MGS_OK;
+  const size_t w = mgs::dtype_bytes(dtype);
+  if (!d_out) return invalid("mgs_generate_device: d_out is null");
+  if (reinterpret_cast<uintptr_t>(d_out) % w != 0) return invalid("mgs_generate_device: d_out is not key-aligned");
+  if (n > kMaxDeviceSortKeys) return invalid("mgs_generate_device: n must be below 2^32");
+  Context& c = ctx->impl;
+  DeviceGuard g(c.device);
+  if (need > 0) {
+    cudaError_t e = c.reserve(need);
+    if (e != cudaSuccess) return cuda_fail(e, "mgs_generate_device: arena");
+  }
+  cudaError_t e = mgs::generate_device(dtype, distribution, seed, d_out, n, c.arena, c.arena_bytes, c.compute,
+                                       c.d_status, &c.recorder);
+  if (e != cudaSuccess) return cuda_fail(e, "mgs_generate_device");
+  return finish_sync(c, "mgs_generate_device: synchronize");
 }
 
 }  // extern "C"

@@ -23,13 +23,14 @@
 #include <limits>
 #include <parallel/algorithm>
 #include <random>
+#include <sstream>
 #include <string>
 #include <vector>
 
+#include "data_generator.h"
+
 namespace mgs {
 namespace {
-
-constexpr int kGeneratorThreads = 128;  // fixed by the reference scheme (src/data_generator.cuh:210)
 
 // Same seeding procedure as src/data_generator.cuh:193-205: fill a seed
 // sequence as long as the generator state with successive left-rotations of
@@ -261,15 +262,18 @@ void normal0(T* out, size_t n, uint32_t seed) {
 // Zipf(s) over `distinct` ranks by inverse CDF; rank k maps to a fixed scattered
 // key value so that every digit position varies.
 template <typename T>
-void zipf(T* out, size_t n, uint32_t seed, double s, size_t distinct) {
-  std::vector<double> cdf(distinct);
+void zipf_tables_typed(uint32_t seed, double s, size_t distinct, std::vector<double>* cdf_out,
+                       std::vector<T>* value_out) {
+  std::vector<double>& cdf = *cdf_out;
+  cdf.assign(distinct, 0.0);
   double acc = 0.0;
   for (size_t k = 0; k < distinct; ++k) {
     acc += std::pow(double(k + 1), -s);
     cdf[k] = acc;
   }
   for (auto& c : cdf) c /= acc;
-  std::vector<T> value(distinct);
+  std::vector<T>& value = *value_out;
+  value.assign(distinct, T(0));
   for (size_t k = 0; k < distinct; ++k) {
     const uint64_t r = splitmix64(uint64_t(seed) * 0x100000001B3ull + k);
     if (std::is_floating_point<T>::value) {
@@ -278,6 +282,13 @@ void zipf(T* out, size_t n, uint32_t seed, double s, size_t distinct) {
       value[k] = from_bits<T>(r);
     }
   }
+}
+
+template <typename T>
+void zipf(T* out, size_t n, uint32_t seed, double s, size_t distinct) {
+  std::vector<double> cdf;
+  std::vector<T> value;
+  zipf_tables_typed<T>(seed, s, distinct, &cdf, &value);
 #pragma omp parallel for schedule(static)
   for (size_t i = 0; i < n; ++i) {
     const double u = unit(draw(seed, 3, i));
@@ -359,7 +370,7 @@ bool generate_typed(const std::string& dist_in, uint32_t seed, T* out, size_t n)
   } else if (dist == "normal0") {
     normal0<T>(out, n, seed);
   } else if (dist == "zipf") {
-    zipf<T>(out, n, seed, 1.1, size_t(1) << 20);
+    zipf<T>(out, n, seed, kZipfExponent, kZipfDistinct);
   } else if (dist == "sorted-full" || dist == "reverse-sorted-full" || dist == "nearly-sorted-swaps") {
     full_uniform<T>(out, n, seed);
     if (dist == "reverse-sorted-full") {
@@ -377,7 +388,44 @@ bool generate_typed(const std::string& dist_in, uint32_t seed, T* out, size_t n)
   return true;
 }
 
+template <typename T>
+void zipf_tables_bytes(uint32_t seed, std::vector<double>* cdf, std::vector<unsigned char>* bytes) {
+  std::vector<T> value;
+  zipf_tables_typed<T>(seed, kZipfExponent, kZipfDistinct, cdf, &value);
+  bytes->resize(value.size() * sizeof(T));
+  std::memcpy(bytes->data(), value.data(), bytes->size());
+}
+
 }  // namespace
+
+void generator_static_block(size_t n, int t, size_t* begin, size_t* end) { static_block(n, t, begin, end); }
+
+bool mt19937_seed_state(uint32_t seed, uint32_t* state624) {
+  // The engine's textual form is its state: the 624 words, then (libstdc++)
+  // the position of the next output, which is 624 for a freshly seeded engine.
+  std::ostringstream os;
+  os << seeded_generator(seed);
+  std::istringstream is(os.str());
+  for (size_t i = 0; i < std::mt19937::state_size; ++i) {
+    unsigned long long v;
+    if (!(is >> v) || v > 0xFFFFFFFFull) return false;
+    state624[i] = static_cast<uint32_t>(v);
+  }
+  unsigned long long p;
+  return bool(is >> p) && p == std::mt19937::state_size;
+}
+
+bool zipf_tables(int dtype, uint32_t seed, std::vector<double>* cdf, std::vector<unsigned char>* values) {
+  switch (dtype) {
+    case 0: zipf_tables_bytes<uint32_t>(seed, cdf, values); return true;
+    case 1: zipf_tables_bytes<int32_t>(seed, cdf, values); return true;
+    case 2: zipf_tables_bytes<float>(seed, cdf, values); return true;
+    case 3: zipf_tables_bytes<uint64_t>(seed, cdf, values); return true;
+    case 4: zipf_tables_bytes<int64_t>(seed, cdf, values); return true;
+    case 5: zipf_tables_bytes<double>(seed, cdf, values); return true;
+    default: return false;
+  }
+}
 
 // dtype codes follow mgs_dtype (u32, i32, f32, u64, i64, f64).
 bool generate_keys(int dtype, const char* distribution, uint32_t seed, void* out, size_t n) {

@@ -108,6 +108,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
                                    c_void], c_int),
         "mgs_sort_device_noalloc": ([c_int, c_void, c_size, c_void], c_int),
         "mgs_generate": ([c_int, ctypes.c_char_p, c_u32, c_void, c_size], c_int),
+        "mgs_generate_device": ([c_void, c_int, ctypes.c_char_p, c_u32, c_void, c_size], c_int),
         "mgs_tanasic_sort": ([c_void, c_int, c_void, c_size, c_int], c_int),
         "mgs_tanasic_sort_device": ([c_void, c_int, c_void, c_size, c_int], c_int),
         "mgs_find_pivot_device": ([c_void, c_int, ctypes.POINTER(c_void), ctypes.POINTER(c_void), c_int, c_size,
@@ -339,6 +340,12 @@ class Context:
                                                int(begin_bit), int(end_bit), 1 if descending else 0,
                                                ctypes.c_void_p(d_temp or None), int(temp_bytes),
                                                ctypes.c_void_p(stream or None)))
+
+    def generate_device(self, d_out: int, n: int, dtype, distribution: str, seed: int) -> None:
+        """The bytes of generate(dtype, distribution, seed, n), written straight into device memory
+        (mgs_generate_device); refuses the distributions that use the host's log/cos."""
+        _check(self._lib.mgs_generate_device(self.handle, dtype_code(dtype), distribution.encode(),
+                                             int(seed) & 0xFFFFFFFF, ctypes.c_void_p(d_out or None), int(n)))
 
     # --- TanasicSort with one GPU: host buffer in, sorted in place ---
     def sort_host(self, keys: np.ndarray) -> None:
