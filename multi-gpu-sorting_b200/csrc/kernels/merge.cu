@@ -434,18 +434,30 @@ __global__ __launch_bounds__(BLOCK) void tile_merge_kernel(const typename Tr::Bi
 // ---------------------------------------------------------------- host ------
 size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
-template <int KEY_BYTES>
-struct MergeShape;
-template <>
-struct MergeShape<4> {
-  static constexpr int kBlock = 256;
-  static constexpr int kItems = 16;
+// Merge tile shapes: 256, 512 or 1024 threads, each merging 16 (4-byte keys)
+// or 8 (8-byte keys) outputs; a larger tile means fewer tile boundaries to
+// partition and fewer slices per run to stage.
+constexpr int kMergeShapes = 3;
+template <int KEY_BYTES, int SHAPE>
+struct MergeShape {
+  static constexpr int kBlock = 256 << SHAPE;
+  static constexpr int kItems = KEY_BYTES == 4 ? 16 : 8;
 };
-template <>
-struct MergeShape<8> {
-  static constexpr int kBlock = 256;
-  static constexpr int kItems = 8;
-};
+constexpr u64 merge_tile_keys(size_t key_bytes, int shape) { return u64(256 << shape) * (key_bytes == 4 ? 16 : 8); }
+
+// The shape a merge of k runs uses: 256 threads for two runs, 512 for more
+// (measured on a B200, 2^31 u32 keys: k = 2 6.96 ms against 7.53 with 512
+// threads; k = 8 / 32 / 64: 16.27 / 27.50 / 37.48 ms with 256 threads, 16.06 /
+// 26.51 / 34.89 with 512, 17.61 / 27.84 / 35.49 with 1024). MGS_MERGE_SHAPE
+// (0-2) overrides it for experiments.
+int merge_shape(int k) {
+  static const int env = [] {
+    const char* e = getenv("MGS_MERGE_SHAPE");
+    return (e && e[0] >= '0' && e[0] < '0' + kMergeShapes && e[1] == 0) ? e[0] - '0' : -1;
+  }();
+  if (env >= 0) return env;
+  return k <= 2 ? 0 : 1;
+}
 
 constexpr u64 kCoarseTiles = 256;  // fine tiles per coarse diagonal
 
@@ -457,8 +469,7 @@ struct KwayLayout {
 
 template <class Tr>
 KwayLayout kway_layout(int k, size_t total) {
-  using Shape = MergeShape<sizeof(typename Tr::Bits)>;
-  constexpr u64 kTile = u64(Shape::kBlock) * Shape::kItems;
+  const u64 kTile = merge_tile_keys(sizeof(typename Tr::Bits), merge_shape(k));
   KwayLayout L;
   L.num_tiles = (total + kTile - 1) / kTile;
   L.coarse = (k > 2) && (L.num_tiles > 2 * kCoarseTiles);
@@ -497,14 +508,43 @@ cudaError_t launch_partition(LaunchRecorder* rec, int k, dim3 grid, cudaStream_t
 #undef MGS_PARTITION
 }
 
+// The tile-merge launches of one merge, window by window.
+template <class Tr, class Shape>
+cudaError_t launch_tile_merges(const typename Tr::Bits* const* d_runs, int k, const u64* d_splits,
+                               typename Tr::Bits* out, u64 total, u64 num_tiles, size_t window_keys,
+                               const MergeWindowFn& on_window, cudaStream_t stream, LaunchRecorder* rec) {
+  using Bits = typename Tr::Bits;
+  constexpr u64 kTile = u64(Shape::kBlock) * Shape::kItems;
+  auto kernel = tile_merge_kernel<Tr, Shape::kBlock, Shape::kItems>;
+  const size_t bufs = 2 * tile_buffer_elems<Bits>(kTile) * sizeof(Bits);
+  const size_t smem = bufs + size_t(k) * 8 + size_t(2 * (k + 1)) * 4;
+  static SmemLimitOnce attr;
+  cudaError_t e = attr.ensure(kernel, bufs + size_t(kMaxKwayRuns) * 8 + size_t(2 * (kMaxKwayRuns + 1)) * 4);
+  if (e != cudaSuccess) return e;
+  // Output tiles in windows of about window_keys keys (one window when 0).
+  const u64 per_window = window_keys == 0 ? num_tiles : std::max<u64>(1, (u64(window_keys) + kTile - 1) / kTile);
+  for (u64 t0 = 0; t0 < num_tiles; t0 += per_window) {
+    const u64 t1 = std::min<u64>(num_tiles, t0 + per_window);
+    e = launch_kernel(rec, k == 2 ? "merge_tiles" : "kway_merge_tiles", kernel, dim3(unsigned(t1 - t0)),
+                      dim3(Shape::kBlock), smem, stream, d_runs, k, d_splits, out, total, t0);
+    if (e != cudaSuccess) return e;
+    if (on_window) {
+      const u64 first = t0 * kTile, last = std::min<u64>(total, t1 * kTile);
+      e = on_window(size_t(first), size_t(last - first));
+      if (e != cudaSuccess) return e;
+    }
+  }
+  return cudaSuccess;
+}
+
 template <class Tr>
 cudaError_t kway_merge_typed(const void* const* runs_v, const size_t* lens, int k, void* out_v, void* temp,
                              size_t temp_bytes, size_t window_keys, const MergeWindowFn& on_window,
                              cudaStream_t stream, LaunchRecorder* rec) {
   using Bits = typename Tr::Bits;
-  using Shape = MergeShape<sizeof(Bits)>;
-  constexpr u64 kTile = u64(Shape::kBlock) * Shape::kItems;
   if (k <= 0 || k > kMaxKwayRuns) return cudaErrorInvalidValue;
+  const int shape = merge_shape(k);
+  const u64 kTile = merge_tile_keys(sizeof(Bits), shape);
   size_t total = 0;
   for (int r = 0; r < k; ++r) total += lens[r];
   if (total == 0) return cudaSuccess;
@@ -564,28 +604,19 @@ cudaError_t kway_merge_typed(const void* const* runs_v, const size_t* lens, int 
                              static_cast<u64*>(nullptr), static_cast<u64*>(nullptr), static_cast<Bits*>(nullptr));
   }
   if (e != cudaSuccess) return e;
-  auto kernel = tile_merge_kernel<Tr, Shape::kBlock, Shape::kItems>;
-  const size_t bufs = 2 * tile_buffer_elems<Bits>(kTile) * sizeof(Bits);
-  const size_t smem = bufs + size_t(k) * 8 + size_t(2 * (k + 1)) * 4;
-  static SmemLimitOnce attr;
-  e = attr.ensure(kernel, bufs + size_t(kMaxKwayRuns) * 8 + size_t(2 * (kMaxKwayRuns + 1)) * 4);
-  if (e != cudaSuccess) return e;
-  // Output tiles in windows of about window_keys keys (one window when 0).
-  const u64 per_window =
-      window_keys == 0 ? L.num_tiles : std::max<u64>(1, (u64(window_keys) + kTile - 1) / kTile);
-  for (u64 t0 = 0; t0 < L.num_tiles; t0 += per_window) {
-    const u64 t1 = std::min<u64>(L.num_tiles, t0 + per_window);
-    e = launch_kernel(rec, k == 2 ? "merge_tiles" : "kway_merge_tiles", kernel, dim3(unsigned(t1 - t0)),
-                      dim3(Shape::kBlock), smem, stream, d_runs, k, static_cast<const u64*>(d_splits), out, u64(total),
-                      t0);
-    if (e != cudaSuccess) return e;
-    if (on_window) {
-      const u64 first = t0 * kTile, last = std::min<u64>(u64(total), t1 * kTile);
-      e = on_window(size_t(first), size_t(last - first));
-      if (e != cudaSuccess) return e;
-    }
+  const Bits* const* cruns = d_runs;
+  const u64* csplits = d_splits;
+  switch (shape) {
+    case 0:
+      return launch_tile_merges<Tr, MergeShape<sizeof(Bits), 0>>(cruns, k, csplits, out, u64(total), L.num_tiles,
+                                                                 window_keys, on_window, stream, rec);
+    case 1:
+      return launch_tile_merges<Tr, MergeShape<sizeof(Bits), 1>>(cruns, k, csplits, out, u64(total), L.num_tiles,
+                                                                 window_keys, on_window, stream, rec);
+    default:
+      return launch_tile_merges<Tr, MergeShape<sizeof(Bits), 2>>(cruns, k, csplits, out, u64(total), L.num_tiles,
+                                                                 window_keys, on_window, stream, rec);
   }
-  return cudaSuccess;
 }
 
 template <class Tr>
