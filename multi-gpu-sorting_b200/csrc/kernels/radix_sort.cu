@@ -217,7 +217,7 @@ template <typename V>
 constexpr bool kHasValues = !std::is_same<V, NoValue>::value;
 template <typename V, int N>
 struct ValueTiles {
-  alignas(16) V v[2][N];  // the values of the two key buffers
+  alignas(16) V v[2][N + 16 / sizeof(V)];  // the values of the two key buffers (+ 16 bytes: aligned window)
 };
 template <int N>
 struct ValueTiles<NoValue, N> {};
@@ -227,7 +227,9 @@ struct OnesweepSmem {
   static constexpr int kTile = BLOCK * ITEMS;
   static constexpr int kWarps = BLOCK / 32;
   static constexpr int kChains = kWarps * CHAINS;  // ranking chains (CHAINS per warp)
-  typename Tr::Bits keys[2][kTile];    // double buffer: tile being sorted / next tile in flight
+  // Double buffer: tile being sorted / next tile in flight. A tile arrives as
+  // the 16-byte-aligned window that covers it, so a row holds 16 bytes more.
+  alignas(16) typename Tr::Bits keys[2][kTile + 16 / sizeof(typename Tr::Bits)];
   ValueTiles<V, kTile> vals;
   uint32_t ccount[kChains * kRadix];     // per-chain digit counters -> tile positions
   uint32_t masks[kChains * 2 * kRadix];  // per-chain peer masks (shared-memory multisplit)
@@ -527,6 +529,30 @@ __device__ __forceinline__ TileSpan<Tr> seg_span(const SegLarge& sg, const typen
   return sp;
 }
 
+// The 16-byte-aligned window that covers [p, p + count): it starts at p
+// rounded down to 16 bytes and ends at p + count rounded up (the bulk copy's
+// alignment rule), and the tile starts `shift` elements into it. ok only when
+// the window lies inside the array [lo, hi).
+template <typename T>
+struct AlignedWindow {
+  const T* start;
+  uint32_t bytes;
+  uint32_t shift;
+  bool ok;
+};
+template <typename T>
+__device__ __forceinline__ AlignedWindow<T> aligned_window(const T* p, uint32_t count, const T* lo, const T* hi) {
+  const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+  const uintptr_t a0 = a & ~uintptr_t(15);
+  const uintptr_t e1 = (a + uintptr_t(count) * sizeof(T) + 15) & ~uintptr_t(15);
+  AlignedWindow<T> w;
+  w.start = reinterpret_cast<const T*>(a0);
+  w.bytes = uint32_t(e1 - a0);
+  w.shift = uint32_t((a - a0) / sizeof(T));
+  w.ok = a0 >= reinterpret_cast<uintptr_t>(lo) && e1 <= reinterpret_cast<uintptr_t>(hi);
+  return w;
+}
+
 // vbuf0/vbuf1: the value buffers of buf0/buf1 (key-value sort), else null.
 template <class Tr, int BLOCK, int ITEMS, int MINB, int CHAINS, typename StatusT, int MATCH, bool SEG,
           typename V = NoValue, class Dg = PlainDigits>
@@ -541,8 +567,6 @@ __global__ __launch_bounds__(BLOCK, MINB) void radix_onesweep_kernel(typename Tr
   static_assert(!(SEG && kHasValues<V>), "the segmented sort carries no values");
   constexpr int kTile = Smem::kTile;
   constexpr int kChains = Smem::kChains;
-  constexpr uint32_t kKeyBytes = uint32_t(kTile * sizeof(Bits));
-  constexpr uint32_t kTileBytes = kKeyBytes + (kHasValues<V> ? uint32_t(kTile * sizeof(V)) : 0u);
   static_assert(BLOCK >= kRadix, "one thread per digit");
   extern __shared__ __align__(128) unsigned char smem_raw[];
   Smem& sm = *reinterpret_cast<Smem*>(smem_raw);
@@ -566,19 +590,36 @@ __global__ __launch_bounds__(BLOCK, MINB) void radix_onesweep_kernel(typename Tr
     TileSpan<Tr> sp{src, dst, 0u, n, st->bucket_start[pass]};
     return sp;
   };
-  auto tma_ok = [&](const TileSpan<Tr>& sp, uint32_t t) {
-    const size_t off = size_t(t - sp.first_tile) * kTile;
-    bool ok = use_tma && off + kTile <= sp.seg_len && ((reinterpret_cast<uintptr_t>(sp.src + off) & 15u) == 0);
-    if constexpr (kHasValues<V>) ok = ok && ((reinterpret_cast<uintptr_t>(vspan.src + off) & 15u) == 0);
-    return ok;
+  // Tile t's keys (and values) as aligned windows of the source arrays. The
+  // keys of a segment or of an unaligned buffer start anywhere; the window
+  // copy still goes through the TMA, and the tile is read `shift` keys into
+  // the buffer. Only a window that would leave the array (the first or last
+  // tile of an unaligned array) takes plain loads.
+  struct Windows {
+    AlignedWindow<Bits> k;
+    AlignedWindow<V> v;
+    bool tma;
   };
-  // One tile's keys (and values) into buffer b with the TMA, completing on bar[b].
-  auto issue_copy = [&](int b, const TileSpan<Tr>& sp, uint32_t t) {
+  auto windows_of = [&](const TileSpan<Tr>& sp, uint32_t t) {
     const size_t off = size_t(t - sp.first_tile) * kTile;
-    mbar_arrive_expect_tx(&sm.bar[b], kTileBytes);
-    bulk_copy_g2s(sm.keys[b], sp.src + off, kKeyBytes, &sm.bar[b]);
-    if constexpr (kHasValues<V>)
-      bulk_copy_g2s(sm.vals.v[b], vspan.src + off, uint32_t(kTile * sizeof(V)), &sm.bar[b]);
+    const uint32_t count = uint32_t(min(size_t(kTile), size_t(sp.seg_len) - off));
+    Windows w;
+    w.k = aligned_window<Bits>(sp.src + off, count, src, src + n);
+    w.tma = use_tma && w.k.ok;
+    if constexpr (kHasValues<V>) {
+      const size_t voff = size_t(sp.src - src) + off;
+      w.v = aligned_window<V>(vspan.src + voff, count, vspan.src, vspan.src + n);
+      w.tma = w.tma && w.v.ok;
+    } else {
+      w.v = AlignedWindow<V>{nullptr, 0u, 0u, true};
+    }
+    return w;
+  };
+  // One tile's windows into buffer b with the TMA, completing on bar[b].
+  auto issue_copy = [&](int b, const Windows& w) {
+    mbar_arrive_expect_tx(&sm.bar[b], w.k.bytes + (kHasValues<V> ? w.v.bytes : 0u));
+    bulk_copy_g2s(sm.keys[b], w.k.start, w.k.bytes, &sm.bar[b]);
+    if constexpr (kHasValues<V>) bulk_copy_g2s(sm.vals.v[b], w.v.start, w.v.bytes, &sm.bar[b]);
   };
 
   // Persistent CTA: tiles come in launch order from an atomic counter; the
@@ -598,7 +639,8 @@ __global__ __launch_bounds__(BLOCK, MINB) void radix_onesweep_kernel(typename Tr
     if (t < num_tiles) {
       const TileSpan<Tr> sp = span_of(t);
       spans[0] = sp;
-      if (tma_ok(sp, t)) issue_copy(0, sp, t);
+      const Windows w = windows_of(sp, t);
+      if (w.tma) issue_copy(0, w);
     }
   }
   __syncthreads();
@@ -613,30 +655,34 @@ __global__ __launch_bounds__(BLOCK, MINB) void radix_onesweep_kernel(typename Tr
       if (t < num_tiles) {
         const TileSpan<Tr> sp = span_of(t);
         spans[cur ^ 1] = sp;
-        if (tma_ok(sp, t)) {
+        const Windows w = windows_of(sp, t);
+        if (w.tma) {
           asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-          issue_copy(cur ^ 1, sp, t);
+          issue_copy(cur ^ 1, w);
         }
       }
     }
     const TileSpan<Tr> span = spans[cur];
-    Bits* skeys = sm.keys[cur];
     const size_t base = size_t(tile - span.first_tile) * kTile;
     const uint32_t valid = uint32_t(min(size_t(kTile), size_t(span.seg_len) - base));
-    if (tma_ok(span, tile)) {
+    const Windows win = windows_of(span, tile);
+    Bits* skeys = sm.keys[cur];
+    V* svals = nullptr;
+    if constexpr (kHasValues<V>) svals = sm.vals.v[cur];
+    if (win.tma) {
       const bool arrived = mbar_wait_bounded(&sm.bar[cur], (parity >> cur) & 1u, kTmaWaitLimit);
       parity ^= 1u << cur;
       if (__syncthreads_or(!arrived)) {  // block-uniform exit when the copy never completed
         if (tid == 0) atomicOr(&st->error, kStatusTmaTimeout);
         return;
       }
+      skeys += win.k.shift;
+      if constexpr (kHasValues<V>) svals += win.v.shift;
     } else {
       for (uint32_t i = tid; i < valid; i += BLOCK) skeys[i] = span.src[base + i];
       if constexpr (kHasValues<V>)
-        for (uint32_t i = tid; i < valid; i += BLOCK) sm.vals.v[cur][i] = vspan.src[base + i];
+        for (uint32_t i = tid; i < valid; i += BLOCK) svals[i] = vspan.src[size_t(span.src - src) + base + i];
     }
-    V* svals = nullptr;
-    if constexpr (kHasValues<V>) svals = sm.vals.v[cur];
     if (valid == uint32_t(kTile)) {
       onesweep_tile<Tr, BLOCK, ITEMS, CHAINS, StatusT, MATCH, true>(sm, skeys, st, lb_cur, span, tile, valid, pass,
                                                                     svals, vspan, dg);

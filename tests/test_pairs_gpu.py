@@ -105,6 +105,24 @@ def test_argsort_matches_oracle(ctx, mgs, orc, dtype, ib):
     assert k[idx.astype(np.int64)].tobytes() == wk.tobytes()
 
 
+@pytest.mark.parametrize("dtype", ["u32", "f64"])
+@pytest.mark.parametrize("vb", [4, 8])
+@pytest.mark.parametrize("koff,voff", [(1, 0), (0, 1), (3, 1), (2, 3)])
+def test_sort_pairs_unaligned_buffers(ctx, mgs, orc, dtype, vb, koff, voff):
+    """Keys and values at element offsets that are not 16-byte aligned (each on its own shift)."""
+    n = 3 * 16384 + 77
+    k = keys(mgs, dtype, n, 51)
+    v = values(n, vb, 52)
+    tk = to_device(np.concatenate([np.zeros(koff, k.dtype), k]))
+    tv = to_device(np.concatenate([np.zeros(voff, v.dtype), v]))
+    torch.cuda.synchronize()
+    ctx.sort_pairs_device(tk.data_ptr() + koff * k.dtype.itemsize, tv.data_ptr() + voff * vb, vb, n, dtype)
+    ctx.synchronize()
+    wk, wv = orc.sort_pairs(k, v)
+    assert from_device(tk, k.dtype)[koff:].tobytes() == wk.tobytes()
+    assert from_device(tv, v.dtype)[voff:].tobytes() == wv.tobytes()
+
+
 def test_sort_pairs_large_argsort_properties(ctx, mgs):
     """2^26 u32 keys: the argsort's indices gather the input into ascending order, ties by position."""
     n = 1 << 26

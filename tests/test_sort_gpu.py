@@ -60,10 +60,12 @@ def test_sort_device_distributions(ctx, mgs, orc, dtype, dist, n):
 
 
 @pytest.mark.parametrize("dtype", ["u32", "f32", "u64", "f64"])
-@pytest.mark.parametrize("offset", [1, 3])
-def test_sort_device_unaligned_keys(ctx, mgs, orc, dtype, offset):
-    # keys not 16-byte aligned: the tile loads cannot use TMA bulk copies
-    a = keys_for(mgs, dtype, "full-uniform", 100003)
+@pytest.mark.parametrize("offset", [1, 2, 3])
+@pytest.mark.parametrize("n", [100003, 3 * 20480 + 5, 4 * 20480])
+def test_sort_device_unaligned_keys(ctx, mgs, orc, dtype, offset, n):
+    # keys not 16-byte aligned: tiles arrive as the 16-byte-aligned windows that cover them, read from an
+    # offset in shared memory; a window that would leave the array (first or last tile) takes plain loads
+    a = keys_for(mgs, dtype, "full-uniform", n)
     assert device_sort(ctx, mgs, a, dtype, offset=offset).tobytes() == orc.sort(a).tobytes()
 
 
