@@ -291,12 +291,17 @@ __device__ __forceinline__ uint32_t ballot_peers(uint32_t d, bool ok) {
 // synchronizes before reading dst.
 // With values, src_val/dst_val are the value buffers of src/dst: every value
 // goes to the slot its key goes to.
-template <class Tr, int BLOCK, int ITEMS, int CHAINS, int MATCH, bool FULL, bool ALLOW_SKIP, typename V, class OnCounts,
-          class Between, class Dg = PlainDigits>
+// With SPREAD (partial tiles, one chain per warp) the keys may be spread
+// thinner: warp w owns positions [w*32*warp_items, (w+1)*32*warp_items), so
+// that a short tile keeps every warp busy, and a warp stops at its first item
+// that lies wholly past `valid`. Without it the code is the fixed-span form
+// the onesweep kernel is tuned on.
+template <class Tr, int BLOCK, int ITEMS, int CHAINS, int MATCH, bool FULL, bool ALLOW_SKIP, bool SPREAD = false,
+          typename V = NoValue, class OnCounts = void, class Between = void, class Dg = PlainDigits>
 __device__ __forceinline__ bool rank_tile(OnesweepSmem<Tr, BLOCK, ITEMS, CHAINS, V>& sm, const typename Tr::Bits* src,
                                           typename Tr::Bits* dst, uint32_t valid, int pass, uint32_t* tile_count_out,
                                           OnCounts on_counts, Between between, const V* src_val = nullptr,
-                                          V* dst_val = nullptr, Dg dg = Dg{}) {
+                                          V* dst_val = nullptr, Dg dg = Dg{}, uint32_t warp_items = ITEMS) {
   using Bits = typename Tr::Bits;
   constexpr int kTile = BLOCK * ITEMS;
   constexpr int kChains = (BLOCK / 32) * CHAINS;
@@ -305,7 +310,11 @@ __device__ __forceinline__ bool rank_tile(OnesweepSmem<Tr, BLOCK, ITEMS, CHAINS,
   static_assert(MATCH == 2 || MATCH == 3, "ranking modes: shared-memory masks, or half ballots");
   const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
-  const int wbase = warp * 32 * ITEMS;
+  constexpr bool kSpread = SPREAD && !FULL && CHAINS == 1;
+  const int witems = kSpread ? int(warp_items) : ITEMS;
+  const int wbase = warp * 32 * witems;
+  // Warp-uniform: item i of this warp holds no key of the tile.
+  auto item_done = [&](int i) { return kSpread && (i >= witems || uint32_t(wbase + i * 32) >= valid); };
 
   for (int i = tid; i < kChains * kRadix; i += BLOCK) sm.ccount[i] = 0u;
   __syncthreads();
@@ -314,6 +323,7 @@ __device__ __forceinline__ bool rank_tile(OnesweepSmem<Tr, BLOCK, ITEMS, CHAINS,
   V val[kHasValues<V> ? ITEMS : 1];
 #pragma unroll
   for (int i = 0; i < ITEMS; ++i) {
+    if (item_done(i)) break;  // positions grow with i: the rest lie past `valid` too
     const uint32_t idx = wbase + i * 32 + lane;
     key[i] = src[idx];
     if constexpr (kHasValues<V>) val[i] = src_val[idx];
@@ -353,6 +363,7 @@ __device__ __forceinline__ bool rank_tile(OnesweepSmem<Tr, BLOCK, ITEMS, CHAINS,
   const uint32_t lmask_gt = lanemask_gt();
 #pragma unroll
   for (int j = 0; j < kPerChain; ++j) {
+    if (item_done(j)) break;  // chain 0's item j comes first: every chain's item j lies past `valid`
     uint32_t d[CHAINS], peers[CHAINS], pos[CHAINS];
     bool ok[CHAINS];
     uint32_t* cc[CHAINS];
@@ -875,11 +886,13 @@ __global__ __launch_bounds__(BLOCK, MINB) void seg_small_medium_kernel(typename 
       const uint32_t len = uint32_t(offsets[seg + 1] - b);
       Bits* g = keys + b;
       for (uint32_t i = tid; i < len; i += BLOCK) sm.keys[0][i] = g[i];
+      const uint32_t span = (len + BLOCK - 1) / BLOCK;  // keys per lane: every warp takes a share
       int cur = 0;
       for (int pass = 0; pass < Tr::kPasses; ++pass) {
         uint32_t tc;
-        const bool skipped = rank_tile<Tr, BLOCK, ITEMS, CHAINS, MATCH, false, true>(
-            sm, sm.keys[cur], sm.keys[cur ^ 1], len, pass, &tc, [](uint32_t) {}, [](uint32_t) {});
+        const bool skipped = rank_tile<Tr, BLOCK, ITEMS, CHAINS, MATCH, false, true, true>(
+            sm, sm.keys[cur], sm.keys[cur ^ 1], len, pass, &tc, [](uint32_t) {}, [](uint32_t) {},
+            static_cast<const NoValue*>(nullptr), static_cast<NoValue*>(nullptr), PlainDigits{}, span);
         __syncthreads();
         if (!skipped) cur ^= 1;
       }

@@ -51,6 +51,22 @@ def test_mixed_size_classes(ctx, mgs, orc, dtype, seed):
     assert got.tobytes() == orc.segmented_sort(a, offs).tobytes()
 
 
+@pytest.mark.parametrize("dtype", TYPES)
+def test_medium_segments_spread_over_warps(ctx, mgs, orc, dtype):
+    """One-CTA segments of every length class: keys per lane 1, 2, ... up to a whole tile, the last
+    warp's share partial or empty."""
+    rng = np.random.default_rng(8)
+    lengths = np.array([257, 300, 511, 512, 513, 1000, 1023, 1024, 1025, 2047, 2049, 4096, 5000, 8191, 8192,
+                        8193, 12345, 16383, 16384] * 3)
+    rng.shuffle(lengths)
+    offs = layout(rng, lengths)
+    n = int(offs[-1])
+    dist = "full-uniform-specials" if mgs.np_dtype(dtype).kind == "f" else "zipf"
+    a = mgs.generate(dtype, dist, 21, n)
+    got = run_segmented(ctx, mgs, a, offs, dtype)
+    assert got.tobytes() == orc.segmented_sort(a, offs).tobytes()
+
+
 @pytest.mark.parametrize("dtype", ["u32", "f32", "u64"])
 def test_zipf_segment_lengths(ctx, mgs, orc, dtype):
     """10^4 segments, Zipf(1.2) lengths in [1, 2^22] scaled to ~2^24 keys, random order."""
