@@ -248,7 +248,7 @@ constexpr size_t tile_buffer_elems(size_t tile) {
 }
 
 template <class Tr, int BLOCK, int ITEMS>
-__global__ __launch_bounds__(BLOCK) void tile_merge_kernel(const typename Tr::Bits* const* __restrict__ runs, int k,
+__global__ __launch_bounds__(BLOCK, BLOCK == 256 ? 5 : BLOCK == 512 ? 3 : 1) void tile_merge_kernel(const typename Tr::Bits* const* __restrict__ runs, int k,
                                                            const u64* __restrict__ splits,
                                                            typename Tr::Bits* __restrict__ out, u64 total, u64 tile0) {
   using Bits = typename Tr::Bits;
