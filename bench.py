@@ -180,6 +180,16 @@ def batched_bench(mgs, torch, ctx):
     ctx.synchronize()
     batched_ms = statistics.median(times)
     direct_result = work.clone()
+    # one more call with the library's per-launch CUDA events on, outside the timed runs: time per kernel
+    ctx.set_profiling(True)
+    ctx.kernel_times()  # clear
+    with torch.cuda.stream(stream):
+        work.copy_(pristine)
+        ctx.segmented_sort_device(work.data_ptr(), n, d_offs.data_ptr(), offs.size - 1, "u32", temp.data_ptr(),
+                                  temp_bytes, stream.cuda_stream)
+    stream.synchronize()
+    kernel_ms = {name: {"launches": c, "total_ms": t} for name, (c, t) in ctx.kernel_times().items()}
+    ctx.set_profiling(False)
     # the same launches recorded once into a CUDA graph (mgs_plan_segmented_create) and replayed
     graph_ms, graph_same = replay_ms(ctx, torch, stream, work, pristine, direct_result,
                                      lambda: ctx.plan_segmented(work.data_ptr(), n, d_offs.data_ptr(), offs.size - 1,
@@ -209,7 +219,7 @@ def batched_bench(mgs, torch, ctx):
             "batched_ms": batched_ms, "batched_keys_per_s": n / (batched_ms / 1e3),
             "plain_ms": plain_ms, "plain_keys_per_s": n / (plain_ms / 1e3),
             "speedup_vs_plain": plain_ms / batched_ms,
-            "graph_ms": graph_ms, "graph_same_result": graph_same, "small_batch": small}
+            "graph_ms": graph_ms, "graph_same_result": graph_same, "small_batch": small, "kernel_ms": kernel_ms}
 
 
 def replay_ms(ctx, torch, stream, work, pristine, expected, make_plan, reps):
