@@ -108,9 +108,9 @@ def test_argsort_matches_oracle(ctx, mgs, orc, dtype, ib):
 @pytest.mark.parametrize("dtype", ["u32", "f64"])
 @pytest.mark.parametrize("vb", [4, 8])
 @pytest.mark.parametrize("koff,voff", [(1, 0), (0, 1), (3, 1), (2, 3)])
-def test_sort_pairs_unaligned_buffers(ctx, mgs, orc, dtype, vb, koff, voff):
+@pytest.mark.parametrize("n", [3, 8193, 3 * 16384 + 77])
+def test_sort_pairs_unaligned_buffers(ctx, mgs, orc, dtype, vb, koff, voff, n):
     """Keys and values at element offsets that are not 16-byte aligned (each on its own shift)."""
-    n = 3 * 16384 + 77
     k = keys(mgs, dtype, n, 51)
     v = values(n, vb, 52)
     tk = to_device(np.concatenate([np.zeros(koff, k.dtype), k]))

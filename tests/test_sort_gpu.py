@@ -61,7 +61,7 @@ def test_sort_device_distributions(ctx, mgs, orc, dtype, dist, n):
 
 @pytest.mark.parametrize("dtype", ["u32", "f32", "u64", "f64"])
 @pytest.mark.parametrize("offset", [1, 2, 3])
-@pytest.mark.parametrize("n", [100003, 3 * 20480 + 5, 4 * 20480])
+@pytest.mark.parametrize("n", [1, 5, 4097, 20481, 100003, 3 * 20480 + 5, 4 * 20480])
 def test_sort_device_unaligned_keys(ctx, mgs, orc, dtype, offset, n):
     # keys not 16-byte aligned: tiles arrive as the 16-byte-aligned windows that cover them, read from an
     # offset in shared memory; a window that would leave the array (first or last tile) takes plain loads
