@@ -431,7 +431,10 @@ struct ValueSpan {
 // the look-back as soon as they are known), look back over the segment's
 // earlier tiles while the other warps rank, scatter the digit runs (with their
 // values, svals being the tile's value buffer, when V is a value type).
-template <class Tr, int BLOCK, int ITEMS, int CHAINS, typename StatusT, int MATCH, bool FULL, typename V, class Dg>
+// SPREAD: a partial tile is ranked over all warps (ceil(valid / BLOCK) keys per
+// lane), as the segmented sort's many short last tiles want.
+template <class Tr, int BLOCK, int ITEMS, int CHAINS, typename StatusT, int MATCH, bool FULL, bool SPREAD, typename V,
+          class Dg>
 __device__ __forceinline__ void onesweep_tile(OnesweepSmem<Tr, BLOCK, ITEMS, CHAINS, V>& sm, typename Tr::Bits* skeys,
                                               RadixState* __restrict__ st, StatusT* __restrict__ lb_cur,
                                               const TileSpan<Tr>& span, uint32_t tile, uint32_t valid, int pass,
@@ -446,7 +449,8 @@ __device__ __forceinline__ void onesweep_tile(OnesweepSmem<Tr, BLOCK, ITEMS, CHA
   // round. With 512 threads the other eight warps rank their keys meanwhile, so
   // the waits on other tiles overlap ranking.
   uint32_t tile_count = 0;
-  rank_tile<Tr, BLOCK, ITEMS, CHAINS, MATCH, FULL, false>(
+  const uint32_t warp_items = (SPREAD && !FULL) ? (valid + BLOCK - 1) / BLOCK : uint32_t(ITEMS);
+  rank_tile<Tr, BLOCK, ITEMS, CHAINS, MATCH, FULL, false, SPREAD>(
       sm, skeys, skeys, valid, pass, &tile_count,
       [&](uint32_t count) {
         StatusT* slot = lb_cur + size_t(tile) * kRadix + tid;
@@ -492,7 +496,7 @@ __device__ __forceinline__ void onesweep_tile(OnesweepSmem<Tr, BLOCK, ITEMS, CHA
         }
         sm.gbase[tid] = span.bucket[tid] + uint32_t(excl) - sm.tile_start[tid];
       },
-      svals, svals, dg);
+      svals, svals, dg, warp_items);
   __syncthreads();
 
   // Phase 3: consecutive threads write consecutive positions of one digit run.
@@ -518,17 +522,13 @@ struct SegLarge {
   const uint32_t* tile_prefix;        // first global tile of each large segment (n_large + 1)
   const uint32_t* counts;             // [n_small, n_medium, n_large, large_tiles]
   const uint32_t* bucket;             // [n_large][P][256] bucket starts
+  const uint32_t* tile_seg;           // large segment (index into ids) of every large tile
 };
 
 template <class Tr>
 __device__ __forceinline__ TileSpan<Tr> seg_span(const SegLarge& sg, const typename Tr::Bits* src,
                                                  typename Tr::Bits* dst, uint32_t tile, int pass) {
-  const uint32_t nl = sg.counts[2];
-  uint32_t lo = 0, hi = nl;  // largest s with tile_prefix[s] <= tile
-  while (hi - lo > 1) {
-    const uint32_t mid = (lo + hi) >> 1;
-    if (sg.tile_prefix[mid] <= tile) lo = mid; else hi = mid;
-  }
+  const uint32_t lo = sg.tile_seg[tile];
   const uint32_t seg = sg.ids[lo];
   const unsigned long long b = sg.offsets[seg];
   TileSpan<Tr> sp;
@@ -641,7 +641,11 @@ __global__ __launch_bounds__(BLOCK, MINB) void radix_onesweep_kernel(typename Tr
   static_assert(sizeof(TileSpan<Tr>) <= sizeof(sm.span[0]), "span slot");
   TileSpan<Tr>* spans = reinterpret_cast<TileSpan<Tr>*>(sm.span);
   for (int i = tid; i < kChains * 2 * kRadix; i += BLOCK) sm.masks[i] = 0u;
-  if (tid == 0) {
+  // The thread that claims tiles and issues their copies. A segment's tile
+  // span takes a few dependent loads; in the segmented sort a thread of the
+  // last warp does it, as the first warps also run the look-back.
+  constexpr int kLeader = SEG ? BLOCK - 32 : 0;
+  if (tid == kLeader) {
     mbar_init(&sm.bar[0], 1);
     mbar_init(&sm.bar[1], 1);
     fence_mbar_init();
@@ -660,7 +664,7 @@ __global__ __launch_bounds__(BLOCK, MINB) void radix_onesweep_kernel(typename Tr
   for (;;) {
     const uint32_t tile = sm.tile_id[cur];
     if (tile >= num_tiles) break;
-    if (tid == 0) {
+    if (tid == kLeader) {
       const uint32_t t = atomicAdd(&st->tile_counter[pass], 1u);
       sm.tile_id[cur ^ 1] = t;
       if (t < num_tiles) {
@@ -695,11 +699,14 @@ __global__ __launch_bounds__(BLOCK, MINB) void radix_onesweep_kernel(typename Tr
         for (uint32_t i = tid; i < valid; i += BLOCK) svals[i] = vspan.src[size_t(span.src - src) + base + i];
     }
     if (valid == uint32_t(kTile)) {
-      onesweep_tile<Tr, BLOCK, ITEMS, CHAINS, StatusT, MATCH, true>(sm, skeys, st, lb_cur, span, tile, valid, pass,
-                                                                    svals, vspan, dg);
+      onesweep_tile<Tr, BLOCK, ITEMS, CHAINS, StatusT, MATCH, true, false>(sm, skeys, st, lb_cur, span, tile, valid,
+                                                                           pass, svals, vspan, dg);
     } else {
-      onesweep_tile<Tr, BLOCK, ITEMS, CHAINS, StatusT, MATCH, false>(sm, skeys, st, lb_cur, span, tile, valid, pass,
-                                                                     svals, vspan, dg);
+      // Partial tiles are spread over all warps in the segmented sort only: the
+      // plain sort has one partial tile per pass, and its kernel keeps the
+      // fixed-span code it is tuned on.
+      onesweep_tile<Tr, BLOCK, ITEMS, CHAINS, StatusT, MATCH, false, SEG>(sm, skeys, st, lb_cur, span, tile, valid,
+                                                                          pass, svals, vspan, dg);
     }
     __syncthreads();
     cur ^= 1;
@@ -910,12 +917,14 @@ __global__ __launch_bounds__(BLOCK, MINB) void seg_small_medium_kernel(typename 
 }
 
 // Per large segment and pass: digit counts (one read of the large segments),
-// and the first look-back array cleared.
+// the segment of every large tile (for the onesweep's tile spans), and the
+// first look-back array cleared.
 template <class Tr, int BLOCK>
 __global__ __launch_bounds__(BLOCK) void seg_histogram_kernel(const typename Tr::Bits* __restrict__ keys,
                                                               SegLarge sg, uint32_t tile,
                                                               uint32_t* __restrict__ seg_hist,
-                                                              uint32_t* __restrict__ lb0) {
+                                                              uint32_t* __restrict__ lb0,
+                                                              uint32_t* __restrict__ tile_seg) {
   using Bits = typename Tr::Bits;
   constexpr int P = Tr::kPasses;
   __shared__ uint32_t h[P * kRadix];
@@ -934,6 +943,7 @@ __global__ __launch_bounds__(BLOCK) void seg_histogram_kernel(const typename Tr:
       }
       s_seg = lo;
       s_first = sg.tile_prefix[lo];
+      tile_seg[t] = lo;
     }
     __syncthreads();
     const uint32_t si = s_seg;
@@ -1305,7 +1315,7 @@ cudaError_t radix_sort_typed(typename Tr::Bits* keys, size_t n, void* temp, size
 // ---------------------------------------------------------------- segmented host
 struct SegLayout {
   size_t state_off, hdr_off, small_off, medium_off, large_off, prefix_off, hist_off, bucket_off, lb0_off, lb1_off,
-      keys_off, total;
+      tile_seg_off, keys_off, total;
   size_t max_large, max_tiles, hist_bytes;
 };
 
@@ -1333,6 +1343,7 @@ SegLayout seg_layout(size_t n, size_t nseg) {
   L.bucket_off = take(L.hist_bytes);
   L.lb0_off = take(L.max_tiles * kRadix * 4);
   L.lb1_off = take(L.max_tiles * kRadix * 4);
+  L.tile_seg_off = take(L.max_tiles * 4);
   L.keys_off = take(n * sizeof(typename Tr::Bits));
   L.total = off;
   return L;
@@ -1360,6 +1371,7 @@ cudaError_t segmented_sort_typed(typename Tr::Bits* keys, size_t n, const uint64
   uint32_t* hist = reinterpret_cast<uint32_t*>(tb + L.hist_off);
   uint32_t* bucket = reinterpret_cast<uint32_t*>(tb + L.bucket_off);
   uint32_t* lb[2] = {reinterpret_cast<uint32_t*>(tb + L.lb0_off), reinterpret_cast<uint32_t*>(tb + L.lb1_off)};
+  uint32_t* tile_seg = reinterpret_cast<uint32_t*>(tb + L.tile_seg_off);
   Bits* tmp = reinterpret_cast<Bits*>(tb + L.keys_off);
   const unsigned long long* offs = reinterpret_cast<const unsigned long long*>(d_offsets);
 
@@ -1382,9 +1394,9 @@ cudaError_t segmented_sort_typed(typename Tr::Bits* keys, size_t n, const uint64
                       static_cast<const uint32_t*>(medium_ids));
     if (e != cudaSuccess) return e;
   }
-  SegLarge sg{offs, large_ids, prefix, hdr->counts, bucket};
+  SegLarge sg{offs, large_ids, prefix, hdr->counts, bucket, tile_seg};
   e = launch_kernel(rec, "seg_histogram", seg_histogram_kernel<Tr, 256>, dim3(unsigned(sms * 4)), dim3(256), 0,
-                    stream, static_cast<const Bits*>(keys), sg, kTile, hist, lb[0]);
+                    stream, static_cast<const Bits*>(keys), sg, kTile, hist, lb[0], tile_seg);
   if (e != cudaSuccess) return e;
   e = launch_kernel(rec, "seg_scan", seg_scan_kernel<Tr::kPasses>, dim3(unsigned(sms * 4)), dim3(kRadix), 0, stream,
                     static_cast<const uint32_t*>(hdr->counts), static_cast<const uint32_t*>(hist), bucket);
