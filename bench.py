@@ -13,14 +13,18 @@ DataGenerator ("uniform" over [0, 2^32), seed 2147483647). Per rank:
           keys) per launch over its CUDA-event time, against the measured HBM
           copy bandwidth.
   cpu_baseline: the reference's CPU sort (the gnu_parallel branch of
-          src/sort_benchmark.cu, compiled from the reference sources into
-          oracle/_ref) on a bounded sample, rank 0 at N=1 only.
+          src/sort_benchmark.cu:103-108, compiled from the reference sources
+          into oracle/_ref) on the same 2^30 keys, a few runs bounded by a
+          time budget, rank 0 at N=1 only.
 With torchrun (N>1) every rank sorts its own 2^30 keys on its own GPU (the path
 shards into independent partitions; no data-path collective): weak scaling,
 value = all ranks' keys / the slowest rank's time.
 
 --impl reference times the reference's CPU implementation of the path (same
-metric and workload, bounded sample per step) on the host cores; rank 0 only.
+metric, the whole 2^30-key workload per step, keys from the reference's own
+DataGenerator) on all host threads, rank 0 only; beside it, for context, the
+reference's GPU path (TanasicSort with one GPU, and the CUB sort thrust::sort
+dispatches to) on the same keys.
 """
 import argparse
 import json
@@ -152,17 +156,38 @@ def zipf_segment_offsets(rng, nseg=100_000, total=1 << 28, s=1.2, max_len=1 << 2
     return offs
 
 
-def batched_bench(mgs, torch, ctx):
-    """Config 5a: one segmented-sort call over 10^5 Zipf(1.2) segments (~2^28 u32 keys) against the plain form,
-    one mgs_sort_device launch per segment, on the same device-resident keys."""
+def verify_segmented(torch, out, src, d_offs, dtype):
+    """On the device (4-byte keys): out equals src with every segment [offs[s], offs[s+1]) stably sorted on
+    its own, in the sort's order (floats: -0.0 equal to +0.0, NaN by transformed bits). torch sorts (segment,
+    order key) pairs stably and gathers the input bits in that order: the expected output, compared byte for
+    byte."""
+    lens = (d_offs[1:] - d_offs[:-1]).to(torch.int64)
+    seg = torch.repeat_interleave(torch.arange(lens.numel(), device=out.device, dtype=torch.int64), lens)
+    key = order_key(torch, src, dtype)
+    if dtype == "i32":  # signed order key: shift it into [0, 2^32)
+        key = key + (1 << 31)
+    comp = (seg << 32) | key
+    del seg, key
+    idx = torch.sort(comp, stable=True)[1]
+    del comp
+    same = bool(torch.equal(src[idx], out))
+    del idx
+    torch.cuda.empty_cache()
+    return same
+
+
+def batched_bench(mgs, torch, ctx, dtype="u32", with_plain=True):
+    """One segmented-sort call over 10^5 Zipf(1.2) segments (~2^28 keys, uint32 or float32 with -0.0 and NaN)
+    against the plain form, one mgs_sort_device launch sequence per segment, on the same device-resident
+    keys. The direct call's output is checked on the device (verify_segmented)."""
     rng = np.random.default_rng(11)
     offs = zipf_segment_offsets(rng)
     n = int(offs[-1])
-    keys = mgs.generate("u32", "full-uniform", 5, n)
+    keys = mgs.generate(dtype, "full-uniform" + ("-specials" if dtype == "f32" else ""), 5, n)
     pristine = torch.from_numpy(keys.view(np.int32)).cuda()
     work = torch.empty_like(pristine)
     d_offs = torch.from_numpy(offs).cuda()
-    temp_bytes = mgs.Context.segmented_sort_temp_bytes("u32", n, offs.size - 1)
+    temp_bytes = mgs.Context.segmented_sort_temp_bytes(dtype, n, offs.size - 1)
     temp = torch.empty(temp_bytes, dtype=torch.uint8, device="cuda")
     stream = torch.cuda.Stream()
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
@@ -171,7 +196,7 @@ def batched_bench(mgs, torch, ctx):
         with torch.cuda.stream(stream):
             work.copy_(pristine)
             ev[0].record(stream)
-            ctx.segmented_sort_device(work.data_ptr(), n, d_offs.data_ptr(), offs.size - 1, "u32", temp.data_ptr(),
+            ctx.segmented_sort_device(work.data_ptr(), n, d_offs.data_ptr(), offs.size - 1, dtype, temp.data_ptr(),
                                       temp_bytes, stream.cuda_stream)
             ev[1].record(stream)
         stream.synchronize()
@@ -179,13 +204,14 @@ def batched_bench(mgs, torch, ctx):
             times.append(ev[0].elapsed_time(ev[1]))
     ctx.synchronize()
     batched_ms = statistics.median(times)
+    verified = verify_segmented(torch, work, pristine, d_offs, dtype)
     direct_result = work.clone()
     # one more call with the library's per-launch CUDA events on, outside the timed runs: time per kernel
     ctx.set_profiling(True)
     ctx.kernel_times()  # clear
     with torch.cuda.stream(stream):
         work.copy_(pristine)
-        ctx.segmented_sort_device(work.data_ptr(), n, d_offs.data_ptr(), offs.size - 1, "u32", temp.data_ptr(),
+        ctx.segmented_sort_device(work.data_ptr(), n, d_offs.data_ptr(), offs.size - 1, dtype, temp.data_ptr(),
                                   temp_bytes, stream.cuda_stream)
     stream.synchronize()
     kernel_ms = {name: {"launches": c, "total_ms": t} for name, (c, t) in ctx.kernel_times().items()}
@@ -193,33 +219,39 @@ def batched_bench(mgs, torch, ctx):
     # the same launches recorded once into a CUDA graph (mgs_plan_segmented_create) and replayed
     graph_ms, graph_same = replay_ms(ctx, torch, stream, work, pristine, direct_result,
                                      lambda: ctx.plan_segmented(work.data_ptr(), n, d_offs.data_ptr(), offs.size - 1,
-                                                                "u32", temp.data_ptr(), temp_bytes), reps=3)
+                                                                dtype, temp.data_ptr(), temp_bytes), reps=3)
     del direct_result
-    small = small_batch_bench(mgs, torch, ctx, stream)
-    # plain form: one sort launch sequence per segment, same stream
-    plain_temp = mgs.Context.sort_temp_bytes("u32", int(np.diff(offs).max()))
-    ptemp = torch.empty(plain_temp, dtype=torch.uint8, device="cuda")
-    base = work.data_ptr()
-    with torch.cuda.stream(stream):
-        work.copy_(pristine)
-        ev[0].record(stream)
-        for s in range(offs.size - 1):
-            length = int(offs[s + 1] - offs[s])
-            if length > 1:
-                ctx.sort_device(base + 4 * int(offs[s]), length, "u32", ptemp.data_ptr(), plain_temp,
-                                stream.cuda_stream)
-        ev[1].record(stream)
-    stream.synchronize()
-    ctx.synchronize()
-    plain_ms = ev[0].elapsed_time(ev[1])
     lens = np.diff(offs)
-    return {"segments": int(offs.size - 1), "keys": n, "dtype": "u32",
-            "lengths": "Zipf(1.2) in [1, 2^22] rescaled to ~2^28 keys, random order",
-            "segments_le_256": int((lens <= 256).sum()), "segments_gt_16384": int((lens > 16384).sum()),
-            "batched_ms": batched_ms, "batched_keys_per_s": n / (batched_ms / 1e3),
-            "plain_ms": plain_ms, "plain_keys_per_s": n / (plain_ms / 1e3),
-            "speedup_vs_plain": plain_ms / batched_ms,
-            "graph_ms": graph_ms, "graph_same_result": graph_same, "small_batch": small, "kernel_ms": kernel_ms}
+    out = {"segments": int(offs.size - 1), "keys": n, "dtype": dtype,
+           "values": "uniform over the full range" + (", 0.1% -0.0 and 0.1% NaN" if dtype == "f32" else ""),
+           "lengths": "Zipf(1.2) in [1, 2^22] rescaled to ~2^28 keys, random order",
+           "segments_le_256": int((lens <= 256).sum()), "segments_gt_16384": int((lens > 16384).sum()),
+           "batched_ms": batched_ms, "batched_keys_per_s": n / (batched_ms / 1e3), "verified": verified,
+           "graph_ms": graph_ms, "graph_same_result": graph_same, "kernel_ms": kernel_ms}
+    if with_plain:
+        out["small_batch"] = small_batch_bench(mgs, torch, ctx, stream)
+        # plain form: one sort launch sequence per segment, same stream
+        plain_temp = mgs.Context.sort_temp_bytes(dtype, int(np.diff(offs).max()))
+        ptemp = torch.empty(plain_temp, dtype=torch.uint8, device="cuda")
+        base = work.data_ptr()
+        with torch.cuda.stream(stream):
+            work.copy_(pristine)
+            ev[0].record(stream)
+            for s in range(offs.size - 1):
+                length = int(offs[s + 1] - offs[s])
+                if length > 1:
+                    ctx.sort_device(base + 4 * int(offs[s]), length, dtype, ptemp.data_ptr(), plain_temp,
+                                    stream.cuda_stream)
+            ev[1].record(stream)
+        stream.synchronize()
+        ctx.synchronize()
+        plain_ms = ev[0].elapsed_time(ev[1])
+        out.update({"plain_ms": plain_ms, "plain_keys_per_s": n / (plain_ms / 1e3),
+                    "speedup_vs_plain": plain_ms / batched_ms})
+        del ptemp
+    del work, pristine, temp, d_offs
+    torch.cuda.empty_cache()
+    return out
 
 
 def replay_ms(ctx, torch, stream, work, pristine, expected, make_plan, reps):
@@ -727,16 +759,51 @@ def cpu_reference_sort(orc, base: np.ndarray, budget_s: float, max_reps: int):
     return base.size / statistics.median(times), threads, times
 
 
+def reference_gpu_path(orc, base: np.ndarray, reps: int = 2):
+    """The reference's own GPU path on the same keys, for context beside the CPU arm: TanasicSort<T> with
+    one GPU (src/tanasic_sort.cuh:223-299: H2D, thrust::sort, D2H; its own sort_phase timer) and the
+    device-resident CUB DeviceRadixSort::SortKeys that thrust::sort dispatches to (CUDA events,
+    src/local_gpu_sort_algorithm_benchmark.cu:51-67). Both come from oracle/_ref only."""
+    import torch
+    n = base.size
+    phase = []
+    work = np.empty_like(base)
+    for _ in range(reps):
+        np.copyto(work, base)
+        orc.ref_tanasic_sort(work, 0)
+        phase.append(orc.ref_phase_seconds("sort_phase"))
+    ok = bool(np.all(work[1:] >= work[:-1]))
+    d_in = torch.from_numpy(base.view(np.int32)).cuda()
+    d_out = torch.empty_like(d_in)
+    _, need = orc.ref_cub_sort_device_ms(0, d_in.data_ptr(), d_out.data_ptr(), n)
+    temp = torch.empty(max(need, 1), dtype=torch.uint8, device="cuda")
+    cub_ms = []
+    for i in range(reps + 3):  # out of place from the same input: every run sorts the same keys
+        torch.cuda.synchronize()
+        ms, _ = orc.ref_cub_sort_device_ms(0, d_in.data_ptr(), d_out.data_ptr(), n, temp.data_ptr(), need)
+        if i >= 3:
+            cub_ms.append(ms)
+    del d_in, d_out, temp
+    sp = statistics.median(phase)
+    cm = statistics.median(cub_ms)
+    return {"tanasic_sort_phase_s": sp, "tanasic_keys_per_s": n / sp, "cub_device_ms": cm,
+            "cub_device_keys_per_s": n / (cm / 1e3), "reps": reps, "sorted": ok,
+            "what": "reference TanasicSort<uint32_t> g=1 (H2D + thrust::sort + D2H, its sort_phase timer) and "
+                    "cub::DeviceRadixSort::SortKeys on device-resident keys (CUDA events), same keys"}
+
+
 def run_reference(args, rank):
+    """The reference arm: the reference's own CPU sort (the gnu_parallel branch of src/sort_benchmark.cu:103-108,
+    compiled from the reference sources into oracle/_ref) on the full workload, every host thread, rank 0 only.
+    The keys come from the reference's own DataGenerator, so nothing of the engine is loaded."""
     if rank != 0:
         return
     orc = load_oracle()
     if not orc.ref_available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref.so not built"}))
         return
-    mgs = load_mgs()
-    sample = 1 << 27
-    base = mgs.generate("u32", "uniform", SEED, sample)
+    n = args.n
+    base = orc.ref_generate(np.uint32, "uniform", SEED, n)
     threads = orc.ref_num_procs()
     work = np.empty_like(base)
     for _ in range(args.warmup):
@@ -746,17 +813,24 @@ def run_reference(args, rank):
     for _ in range(args.steps):
         np.copyto(work, base)
         times.append(orc.ref_gnu_parallel_sort(work, threads))
-    value = sample * len(times) / sum(times)
+    ok = bool(np.all(work[1:] >= work[:-1]))
+    del work
+    value = n * len(times) / sum(times)
+    gpu_path = None
+    if not args.no_reference_gpu:
+        gpu_path = reference_gpu_path(orc, base)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "keys/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
-        "data": "synthetic (reference DataGenerator)",
-        "config": {"workload": WORKLOAD, "sample_keys": sample,
-                   "algorithm": "reference gnu_parallel sort (src/sort_benchmark.cu:314-319), oracle/_ref"},
+        "data": "synthetic (reference DataGenerator, oracle/_ref)",
+        "config": {"workload": WORKLOAD, "keys": n, "same_config": n == N_KEYS, "verified_sorted": ok,
+                   "algorithm": "reference gnu_parallel sort (src/sort_benchmark.cu:103-108), oracle/_ref"},
         "cpu_baseline": {"value": value, "unit": "keys/s", "cores": threads, "kind": "reference",
-                         "sample": f"2^27 of the 2^30 uint32 keys per step, {args.steps} steps"},
+                         "sample": f"the whole workload ({n} uint32 keys) per step, {args.steps} steps, "
+                                   f"{args.warmup} warm-up steps"},
         "e2e": {"value": value, "unit": "keys/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "reference_gpu_path": gpu_path,
     }
     print(json.dumps(line))
 
@@ -772,6 +846,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched (segmented) measurement")
     ap.add_argument("--no-served", action="store_true", help="skip the serving-loop measurement")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="--impl reference: skip timing the reference's GPU path beside its CPU sort")
     ap.add_argument("--sweep", choices=["types", "merge", "ooc", "tune", "pairs", "generate"],
                     help="measure another workload of the sort API instead (one JSON line per case)")
     ap.add_argument("--sweep-n", type=int, default=0, help="keys per case of --sweep (0: the workload's default)")
@@ -837,10 +913,10 @@ def main():
     stream.synchronize()
     ctx.synchronize()
 
-    # verify the warm-up result: sorted and a permutation (sum + histogram)
-    u = work.to(torch.int64) & 0xFFFFFFFF
-    ok = bool((u[1:] >= u[:-1]).all()) and (u.sum() == (pristine.to(torch.int64) & 0xFFFFFFFF).sum()).item()
-    del u
+    # verify the warm-up result on the device: ascending and the same multiset of keys as the input (both
+    # sorted by torch and compared), which for integer keys fixes every output byte
+    ok = verify_sorted_permutation(torch, work, pristine, "u32")
+    torch.cuda.empty_cache()
 
     if world > 1:
         dist.barrier()
@@ -859,6 +935,8 @@ def main():
     ctx.set_profiling(False)
     ctx.synchronize()
     step_ms = [a.elapsed_time(b) for a, b in evs]
+    ok = ok and verify_sorted_permutation(torch, work, pristine, "u32")  # the last timed step's output
+    torch.cuda.empty_cache()
     total_ms = max_over_ranks(dist, world, sum(step_ms), "cuda")
     value = job_keys_per_s(world, n, args.steps, total_ms / 1e3)
 
@@ -897,7 +975,8 @@ def main():
     served = None
     if rank == 0 and world == 1:
         if not args.no_batched:
-            batched = batched_bench(mgs, torch, ctx)
+            batched = {"u32": batched_bench(mgs, torch, ctx, "u32"),
+                       "f32": batched_bench(mgs, torch, ctx, "f32", with_plain=False)}
         if not args.no_served:
             served = served_bench(mgs)
 
@@ -905,11 +984,10 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         orc = load_oracle()
         if orc.ref_available():
-            sample = keys_np[: 1 << 27].copy()
-            v, threads, times = cpu_reference_sort(orc, sample, budget_s=15.0, max_reps=5)
+            v, threads, times = cpu_reference_sort(orc, keys_np, budget_s=12.0, max_reps=3)
             cpu = {"value": v, "unit": "keys/s", "cores": threads, "kind": "reference",
-                   "sample": f"first 2^27 of the 2^30 keys, {len(times)} runs, median "
-                             f"(reference gnu_parallel sort, src/sort_benchmark.cu:314-319)"}
+                   "sample": f"the whole workload ({n} keys), {len(times)} runs, median "
+                             f"(reference gnu_parallel sort, src/sort_benchmark.cu:103-108)"}
 
     if rank == 0:
         line = {

@@ -116,8 +116,11 @@ int mgs_sort_device(mgs_ctx* ctx, int dtype, void* d_keys, size_t n, void* d_tem
  * (2,097,152) keys of 8 bytes; larger n returns MGS_ERR_INVALID. All calls on a GPU share the
  * area: calls that overlap on that GPU race, so order them on one stream. The
  * first call on a device looks up the area's address for that device; make it
- * before any stream capture. Asynchronous on `stream` (a cudaStream_t, NULL =
- * the legacy default stream); device-side timeouts are not reported. */
+ * before any stream capture. After cudaDeviceReset (or any other teardown of
+ * the device's context) the area may move: the next call notices the new
+ * context and looks the address up again, so it counts as a first call again.
+ * Asynchronous on `stream` (a cudaStream_t, NULL = the legacy default
+ * stream); device-side timeouts are not reported. */
 int mgs_sort_device_noalloc(int dtype, void* d_keys, size_t n, void* stream);
 
 /* ---- TanasicSort with one GPU (src/tanasic_sort.cuh:223-299) ------------

@@ -22,9 +22,15 @@
 //     cleared by each call on its stream before use.
 //   * The first call on a device resolves the array's device address for that
 //     device (cudaGetSymbolAddress, with that device current) and caches it.
-//     Make that first call before any stream capture on the device.
+//     Make that first call before any stream capture on the device. The cache
+//     is keyed by the device's current CUDA context (its unique context id):
+//     after cudaDeviceReset, or any other teardown of the device's context,
+//     the library's module is loaded again and the array may sit at a new
+//     address, so the next call resolves it again (that call is then a first
+//     call once more, and must come before any stream capture too).
 //   * Asynchronous on `stream`; device-side wait timeouts are not reported
 //     (there is no context status word), the result is then unspecified.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -43,15 +49,50 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratch
 
 std::mutex g_mutex;
 void* g_scratch_ptr[kMaxDevices] = {};
+unsigned long long g_scratch_ctx[kMaxDevices] = {};  // id of the context the cached address belongs to
 
-// Device address of g_noalloc_scratch on `device` (which is current).
+// Unique id of the calling thread's current CUDA context (ids are never reused
+// within a process), through the driver entry points the runtime exposes; 0
+// when it cannot be read, which forces a fresh address lookup.
+unsigned long long current_context_id() {
+  using GetCurrentFn = CUresult (*)(CUcontext*);
+  using GetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+  static GetCurrentFn get_current = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      f = nullptr;
+    return reinterpret_cast<GetCurrentFn>(f);
+  }();
+  static GetIdFn get_id = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      f = nullptr;
+    return reinterpret_cast<GetIdFn>(f);
+  }();
+  CUcontext c = nullptr;
+  unsigned long long id = 0;
+  if (get_current == nullptr || get_id == nullptr || get_current(&c) != CUDA_SUCCESS || c == nullptr ||
+      get_id(c, &id) != CUDA_SUCCESS)
+    return 0;
+  return id;
+}
+
+// Device address of g_noalloc_scratch on `device` (which is current), looked
+// up again whenever the device's context is not the one the cached address
+// came from.
 cudaError_t scratch_address(int device, void** out) {
   std::lock_guard<std::mutex> lock(g_mutex);
-  if (g_scratch_ptr[device] == nullptr) {
+  const unsigned long long ctx_id = current_context_id();
+  if (g_scratch_ptr[device] == nullptr || ctx_id == 0 || g_scratch_ctx[device] != ctx_id) {
     void* p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess) return e;
     g_scratch_ptr[device] = p;
+    g_scratch_ctx[device] = ctx_id;
   }
   *out = g_scratch_ptr[device];
   return cudaSuccess;

@@ -1,7 +1,7 @@
 // Onesweep LSD radix sort for one B200 (sm_100a): the engine's replacement of
 // thrust::sort -> CUB DeviceRadixSort, which the reference calls for every
 // partition / chunk sort (src/tanasic_sort.cuh:264-266,
-// src/gowanlock_sort.cuh:188-190,337-339, src/sort_benchmark.cu:300).
+// src/gowanlock_sort.cuh:188-190,337-339, src/sort_benchmark.cu:89).
 //
 // Per sort of n keys of w bytes (P = w 8-bit digit passes):
 //   K1 radix_histogram : one streaming read of the keys builds all P digit

@@ -16,8 +16,9 @@
 //
 // Pinned against: the reference's own DataGenerator, gnu-parallel sort,
 // multiway merge and TanasicSort compiled from its sources into oracle/_ref
-// (oracle/Makefile), and golden fixtures in tests/golden produced by the
-// reference's TanasicSort on a B200.
+// (oracle/Makefile). tests/golden holds hashes of the reference
+// DataGenerator's output (tests/golden/make_golden.py); the sort results are
+// compared with the reference's TanasicSort / CUB at test time, on the GPU.
 #include <algorithm>
 #include <cstdint>
 #include <cstring>

@@ -64,7 +64,7 @@ def ref_lib() -> ctypes.CDLL:
         lib.ref_phase_seconds.argtypes = [ctypes.c_char_p]
         lib.ref_phase_seconds.restype = ctypes.c_double
         lib.ref_num_procs.restype = i
-        lib.ref_cub_sort_device_ms.argtypes = [i, v, s, v, s, ctypes.POINTER(s)]
+        lib.ref_cub_sort_device_ms.argtypes = [i, v, v, s, v, s, ctypes.POINTER(s)]
         lib.ref_cub_sort_device_ms.restype = ctypes.c_double
         lib.ref_thrust_sort_by_key.argtypes = [i, v, v, s, s]
         lib.ref_cub_sort_range.argtypes = [i, v, v, s, s, i, i, i]
@@ -194,13 +194,22 @@ def ref_gowanlock_sort(a: np.ndarray, chunk_size: int = 0, merge_group_size: int
                                         device, threads) == 0
 
 
-def ref_cub_sort_device_ms(dtype_code: int, d_keys: int, n: int, d_temp: int = 0, temp_bytes: int = 0):
-    """cub::DeviceRadixSort::SortKeys on device keys (src/local_gpu_sort_algorithm_benchmark.cu:51-67).
-    Returns (ms, temp bytes CUB needs); ms < 0 when only the size was queried."""
+def ref_cub_sort_device_ms(dtype_code: int, d_keys_in: int, d_keys_out: int, n: int, d_temp: int = 0,
+                           temp_bytes: int = 0):
+    """cub::DeviceRadixSort::SortKeys from device keys d_keys_in into d_keys_out (out of place, as CUB requires;
+    src/local_gpu_sort_algorithm_benchmark.cu:51-67). Returns (ms, temp bytes CUB needs); ms < 0 when only the
+    size was queried."""
     need = ctypes.c_size_t()
-    ms = ref_lib().ref_cub_sort_device_ms(dtype_code, ctypes.c_void_p(d_keys), n, ctypes.c_void_p(d_temp or None),
+    ms = ref_lib().ref_cub_sort_device_ms(dtype_code, ctypes.c_void_p(d_keys_in or None),
+                                          ctypes.c_void_p(d_keys_out or None), n, ctypes.c_void_p(d_temp or None),
                                           temp_bytes, ctypes.byref(need))
     return ms, need.value
+
+
+def ref_cub_sort(dtype_code: int, d_keys: int, n: int, w: int) -> None:
+    """The reference's sort order on device keys, in place: cub::DeviceRadixSort::SortKeys over all 8*w bits
+    (the library thrust::sort dispatches to, src/tanasic_sort.cuh:264), run out of place and copied back."""
+    ref_cub_sort_range(dtype_code, d_keys, n, 0, 8 * w, False)
 
 
 def ref_thrust_sort_by_key(dtype_code: int, d_keys: int, d_values: int, value_bytes: int, n: int) -> None:

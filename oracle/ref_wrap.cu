@@ -7,8 +7,8 @@
 //   ref_generate          DataGenerator::ComputeDistribution<T>   src/data_generator.cuh:18-36
 //   ref_tanasic_sort      SetupTanasicSort + TanasicSort<T>        src/tanasic_sort.cuh:206-299
 //   ref_gowanlock_sort    SetupGowanlockSort + GowanlockSort<T>    src/gowanlock_sort.cuh:117-125,395-483
-//   ref_gnu_parallel_sort the "gnu_parallel" algorithm branch      src/sort_benchmark.cu:314-319
-//   ref_multiway_merge    __gnu_parallel::multiway_merge call      src/local_cpu_multiway_merge_benchmark.cu:255-256
+//   ref_gnu_parallel_sort the "gnu_parallel" algorithm branch      src/sort_benchmark.cu:103-108
+//   ref_multiway_merge    __gnu_parallel::multiway_merge call      src/local_cpu_multiway_merge_benchmark.cu:70-71
 //   ref_cub_sort_device_ms cub::DeviceRadixSort::SortKeys on device keys, the
 //                          library call the reference times in
 //                          src/local_gpu_sort_algorithm_benchmark.cu:51-67 (CUDA events)
@@ -222,21 +222,25 @@ int ref_thrust_sort_by_key(int dtype, void* d_keys, void* d_values, size_t value
   });
 }
 
-double ref_cub_sort_device_ms(int dtype, void* d_keys, size_t n, void* d_temp, size_t temp_bytes, size_t* need) {
+// Out of place, as CUB requires (its key ranges must not overlap): d_keys_in is
+// read, d_keys_out receives the sorted keys.
+double ref_cub_sort_device_ms(int dtype, const void* d_keys_in, void* d_keys_out, size_t n, void* d_temp,
+                              size_t temp_bytes, size_t* need) {
   return guarded(-2.0, [&] {
   double ms = -1.0;
   dispatch(dtype, [&](auto tag) {
     using T = decltype(tag);
-    T* p = static_cast<T*>(d_keys);
+    const T* in = static_cast<const T*>(d_keys_in);
+    T* out = static_cast<T*>(d_keys_out);
     size_t bytes = 0;
-    cub::DeviceRadixSort::SortKeys(nullptr, bytes, p, p, n, 0, int(sizeof(T) * 8));
+    cub::DeviceRadixSort::SortKeys(nullptr, bytes, in, out, n, 0, int(sizeof(T) * 8));
     if (need) *need = bytes;
-    if (temp_bytes < bytes || d_temp == nullptr) return;
+    if (temp_bytes < bytes || d_temp == nullptr || in == nullptr || out == nullptr) return;
     cudaEvent_t a, b;
     cudaEventCreate(&a);
     cudaEventCreate(&b);
     cudaEventRecord(a);
-    cub::DeviceRadixSort::SortKeys(d_temp, bytes, p, p, n, 0, int(sizeof(T) * 8));
+    cub::DeviceRadixSort::SortKeys(d_temp, bytes, in, out, n, 0, int(sizeof(T) * 8));
     cudaEventRecord(b);
     cudaEventSynchronize(b);
     float t = 0.f;

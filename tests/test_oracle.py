@@ -30,7 +30,7 @@ def test_sort_matches_reference_gnu_parallel_sort(orc, dt):
         pytest.skip("oracle/_ref not built")
     a = rand(dt, 300001, 5)
     b = a.copy()
-    orc.ref_gnu_parallel_sort(b, 4)  # src/sort_benchmark.cu:314-319
+    orc.ref_gnu_parallel_sort(b, 4)  # src/sort_benchmark.cu:103-108
     assert orc.sort(a).tobytes() == b.tobytes()
 
 

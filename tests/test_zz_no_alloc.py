@@ -75,3 +75,23 @@ def test_noalloc_largest_and_oversized_inputs(ctx, mgs):
     assert fn(0, ctypes.c_void_p(got.data_ptr()), n + 1, ctypes.c_void_p(stream)) == mgs.MGS_ERR_INVALID
     assert b"static scratch" in lib.mgs_last_error_string()
     assert fn(3, ctypes.c_void_p(got.data_ptr()), MAX_KEYS[8] + 1, None) == mgs.MGS_ERR_INVALID
+
+
+def test_noalloc_calls_allocate_no_device_memory(ctx, mgs):
+    """The defining property: once the library's module is loaded on the GPU (the first call), further calls
+    of every size and key width leave the device's free memory unchanged."""
+    lib, fn = noalloc_fn(mgs)
+    cases = [("u32", "uniform", 1 << 22), ("f32", "full-uniform-specials", 100_003), ("u64", "uniform", 1 << 21),
+             ("i64", "zipf", 4097), ("u32", "uniform", 31)]
+    bufs = [(mgs.dtype_code(dt), on_device(mgs.generate(dt, dist, 9, n)), n) for dt, dist, n in cases]
+    stream = torch.cuda.current_stream().cuda_stream
+    code, t, n = bufs[0]
+    assert fn(code, ctypes.c_void_p(t.data_ptr()), n, ctypes.c_void_p(stream)) == mgs.MGS_OK  # warm-up call
+    torch.cuda.synchronize()
+    free_before = torch.cuda.mem_get_info()[0]
+    for _ in range(3):
+        for code, t, n in bufs:
+            assert fn(code, ctypes.c_void_p(t.data_ptr()), n, ctypes.c_void_p(stream)) == mgs.MGS_OK, \
+                lib.mgs_last_error_string()
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free_before
