@@ -347,6 +347,23 @@ int mgs_generate(int dtype, const char* distribution, uint32_t seed, void* out, 
  * when the buffer is filled. n must be below 2^32. */
 int mgs_generate_device(mgs_ctx* ctx, int dtype, const char* distribution, uint32_t seed, void* d_out, size_t n);
 
+/* ---- failure injection for tests (no counterpart in the reference, whose
+ * CheckCudaError ignores errors in release builds, src/cuda_error.cuh:5-10) ----
+ * mgs_test_set_waits: bounds of the sort kernels' device-side waits on
+ * `device` (polls of a look-back status word, polls of a tile-copy barrier;
+ * 0 = the default bound) for sorts launched afterwards, and one tile of the
+ * plain device sort whose look-back status is never published (hold_tile;
+ * 0xFFFFFFFF = none). With a tile held, the look-back after it waits on a word
+ * that nothing sets until its bound runs out; the sort then finishes, its
+ * output unspecified (every write stays inside the keys), and reports
+ * MGS_ERR_TIMEOUT through mgs_ctx_synchronize. Call with (device, 0, 0,
+ * 0xFFFFFFFF) to restore the defaults. Synchronous.
+ * mgs_test_fail_device_allocations: the next `count` growths of any context's
+ * device arena fail as an out-of-memory cudaMalloc would (MGS_ERR_OOM); 0
+ * cancels. */
+int mgs_test_set_waits(int device, uint32_t lookback_spins, uint32_t tma_polls, uint32_t hold_tile);
+int mgs_test_fail_device_allocations(int count);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

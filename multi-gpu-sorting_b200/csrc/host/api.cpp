@@ -865,4 +865,25 @@ int mgs_generate_device(mgs_ctx* ctx, int dtype, const char* distribution, uint3
   return finish_sync(c, "mgs_generate_device: synchronize");
 }
 
+int mgs_test_set_waits(int device, uint32_t lookback_spins, uint32_t tma_polls, uint32_t hold_tile) {
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count) {
+    cudaGetLastError();
+    set_last_error("mgs_test_set_waits: no CUDA device %d", device);
+    return MGS_ERR_NO_DEVICE;
+  }
+  DeviceGuard g(device);
+  const cudaError_t e = mgs::set_wait_control(lookback_spins, tma_polls, hold_tile);
+  if (e != cudaSuccess) return cuda_fail(e, "mgs_test_set_waits");
+  mgs::clear_last_error();
+  return MGS_OK;
+}
+
+int mgs_test_fail_device_allocations(int count) {
+  if (count < 0) return invalid("mgs_test_fail_device_allocations: count must be >= 0");
+  mgs::fail_next_arena_reservations(count);
+  mgs::clear_last_error();
+  return MGS_OK;
+}
+
 }  // extern "C"

@@ -1,5 +1,6 @@
 #include "context.h"
 
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 
@@ -7,7 +8,10 @@ namespace mgs {
 
 namespace {
 thread_local std::string g_last_error;
+std::atomic<int> g_failing_reservations{0};  // arena growths still to fail (test hook)
 }
+
+void fail_next_arena_reservations(int count) { g_failing_reservations.store(count > 0 ? count : 0); }
 
 void set_last_error(const char* fmt, ...) {
   char buf[512];
@@ -77,6 +81,9 @@ cudaError_t EventRecorder::collect(std::vector<std::pair<std::string, std::pair<
 
 cudaError_t Context::reserve(size_t bytes) {
   if (bytes <= arena_bytes) return cudaSuccess;
+  for (int left = g_failing_reservations.load(); left > 0;) {
+    if (g_failing_reservations.compare_exchange_weak(left, left - 1)) return cudaErrorMemoryAllocation;
+  }
   cudaError_t e = cudaDeviceSynchronize();
   if (e != cudaSuccess) return e;
   if (arena) cudaFree(arena);

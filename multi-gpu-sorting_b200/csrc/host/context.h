@@ -15,6 +15,10 @@
 
 namespace mgs {
 
+// Failure injection for tests: the next `count` growths of any context's
+// device arena fail as if cudaMalloc had run out of memory.
+void fail_next_arena_reservations(int count);
+
 // Thread-local last error message of the C ABI.
 void set_last_error(const char* fmt, ...);
 void clear_last_error();

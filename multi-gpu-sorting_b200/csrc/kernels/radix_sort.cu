@@ -90,9 +90,26 @@ struct HistCopies {
   static constexpr int kCopies = Tr::kPasses <= 4 ? 32 : 16;
   static constexpr size_t kSmemBytes = size_t(Tr::kPasses) * kRadix * kCopies * sizeof(uint32_t);
 };
-constexpr uint32_t kLookbackSpinLimit = 1u << 25;
-constexpr uint32_t kTmaWaitLimit = 1u << 24;
+constexpr uint32_t kLookbackSpinLimit = 1u << 25;  // default bound of one look-back wait (polls)
+constexpr uint32_t kTmaWaitLimit = 1u << 24;       // default bound of one tile-copy wait (polls)
+constexpr uint32_t kNoHeldTile = 0xFFFFFFFFu;
 constexpr int kLookahead = 8;  // predecessor statuses fetched per look-back round
+
+// Bounds of the device-side waits and a failure-injection hook, kept in this
+// module's device memory so that a test can change them between sorts
+// (set_wait_control). hold_tile: the plain sort's tile of that id never
+// publishes its look-back status, so the look-back of the tiles after it waits
+// on a word that nothing sets until its bound runs out; the sort then reports
+// a look-back timeout instead of hanging. The output of such a sort is
+// unspecified (every scatter stays inside the array); the next sort is exact
+// again. Default: the bounds above, no tile held.
+struct WaitControl {
+  uint32_t lookback_spins;
+  uint32_t tma_polls;
+  uint32_t hold_tile;
+  uint32_t pad;
+};
+__device__ WaitControl g_wait_control = {kLookbackSpinLimit, kTmaWaitLimit, kNoHeldTile, 0u};
 
 // Look-back status word: 0 = not published yet; (count + 1) with the top bit
 // clear = this tile's own digit count (aggregate); top bit set = inclusive
@@ -438,7 +455,8 @@ template <class Tr, int BLOCK, int ITEMS, int CHAINS, typename StatusT, int MATC
 __device__ __forceinline__ void onesweep_tile(OnesweepSmem<Tr, BLOCK, ITEMS, CHAINS, V>& sm, typename Tr::Bits* skeys,
                                               RadixState* __restrict__ st, StatusT* __restrict__ lb_cur,
                                               const TileSpan<Tr>& span, uint32_t tile, uint32_t valid, int pass,
-                                              V* svals, const ValueSpan<V>& vspan, Dg dg) {
+                                              V* svals, const ValueSpan<V>& vspan, Dg dg, uint32_t spin_limit,
+                                              bool publish) {
   using Bits = typename Tr::Bits;
   using LW = LookbackWord<StatusT>;
   const int tid = threadIdx.x;
@@ -454,7 +472,7 @@ __device__ __forceinline__ void onesweep_tile(OnesweepSmem<Tr, BLOCK, ITEMS, CHA
       sm, skeys, skeys, valid, pass, &tile_count,
       [&](uint32_t count) {
         StatusT* slot = lb_cur + size_t(tile) * kRadix + tid;
-        LW::store(slot, tile == span.first_tile ? (LW::kPrefix | StatusT(count)) : StatusT(count + 1u));
+        if (publish) LW::store(slot, tile == span.first_tile ? (LW::kPrefix | StatusT(count)) : StatusT(count + 1u));
       },
       [&](uint32_t count) {
         if (tid >= kRadix) return;
@@ -485,14 +503,14 @@ __device__ __forceinline__ void onesweep_tile(OnesweepSmem<Tr, BLOCK, ITEMS, CHA
             }
             jt -= used;
             if (!done && used == 0) {
-              if (++spins >= kLookbackSpinLimit) {
+              if (++spins >= spin_limit) {
                 atomicOr(&st->error, kStatusLookbackTimeout);
                 break;
               }
               if (spins > 8) __nanosleep(32);
             }
           }
-          LW::store(lb_cur + size_t(tile) * kRadix + tid, LW::kPrefix | (excl + count));
+          if (publish) LW::store(lb_cur + size_t(tile) * kRadix + tid, LW::kPrefix | (excl + count));
         }
         sm.gbase[tid] = span.bucket[tid] + uint32_t(excl) - sm.tile_start[tid];
       },
@@ -590,6 +608,8 @@ __global__ __launch_bounds__(BLOCK, MINB) void radix_onesweep_kernel(typename Tr
     for (size_t i = size_t(blockIdx.x) * BLOCK + tid; i < words; i += size_t(gridDim.x) * BLOCK) lb_next[i] = 0;
   }
   if (st->skip[pass]) return;  // one digit for every key: identity permutation
+  const WaitControl wc = g_wait_control;
+  const uint32_t held = SEG ? kNoHeldTile : wc.hold_tile;
   int sel = 0;
   for (int q = 0; q < pass; ++q) sel ^= (st->skip[q] == 0u) ? 1 : 0;
   const Bits* src = sel ? buf1 : buf0;
@@ -685,7 +705,7 @@ __global__ __launch_bounds__(BLOCK, MINB) void radix_onesweep_kernel(typename Tr
     V* svals = nullptr;
     if constexpr (kHasValues<V>) svals = sm.vals.v[cur];
     if (win.tma) {
-      const bool arrived = mbar_wait_bounded(&sm.bar[cur], (parity >> cur) & 1u, kTmaWaitLimit);
+      const bool arrived = mbar_wait_bounded(&sm.bar[cur], (parity >> cur) & 1u, wc.tma_polls);
       parity ^= 1u << cur;
       if (__syncthreads_or(!arrived)) {  // block-uniform exit when the copy never completed
         if (tid == 0) atomicOr(&st->error, kStatusTmaTimeout);
@@ -700,13 +720,15 @@ __global__ __launch_bounds__(BLOCK, MINB) void radix_onesweep_kernel(typename Tr
     }
     if (valid == uint32_t(kTile)) {
       onesweep_tile<Tr, BLOCK, ITEMS, CHAINS, StatusT, MATCH, true, false>(sm, skeys, st, lb_cur, span, tile, valid,
-                                                                           pass, svals, vspan, dg);
+                                                                           pass, svals, vspan, dg, wc.lookback_spins,
+                                                                           tile != held);
     } else {
       // Partial tiles are spread over all warps in the segmented sort only: the
       // plain sort has one partial tile per pass, and its kernel keeps the
       // fixed-span code it is tuned on.
       onesweep_tile<Tr, BLOCK, ITEMS, CHAINS, StatusT, MATCH, false, SEG>(sm, skeys, st, lb_cur, span, tile, valid,
-                                                                          pass, svals, vspan, dg);
+                                                                          pass, svals, vspan, dg, wc.lookback_spins,
+                                                                          tile != held);
     }
     __syncthreads();
     cur ^= 1;
@@ -1421,6 +1443,12 @@ cudaError_t segmented_sort_typed(typename Tr::Bits* keys, size_t n, const uint64
 }
 
 }  // namespace
+
+cudaError_t set_wait_control(uint32_t lookback_spins, uint32_t tma_polls, uint32_t hold_tile) {
+  const WaitControl wc{lookback_spins ? lookback_spins : kLookbackSpinLimit, tma_polls ? tma_polls : kTmaWaitLimit,
+                       hold_tile, 0u};
+  return cudaMemcpyToSymbol(g_wait_control, &wc, sizeof(wc));
+}
 
 size_t radix_sort_temp_bytes(int dtype, size_t n) {
   size_t bytes = 0;

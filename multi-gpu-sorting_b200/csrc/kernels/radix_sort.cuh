@@ -13,6 +13,13 @@
 
 namespace mgs {
 
+// Bounds of the radix kernels' device-side waits on the current device (0 =
+// the default bound) and the failure-injection hook: the plain sort's tile
+// `hold_tile` never publishes its look-back status (0xFFFFFFFF: none), so the
+// look-back waits after it run out and the sort reports a timeout. Synchronous;
+// applies to sorts launched afterwards.
+cudaError_t set_wait_control(uint32_t lookback_spins, uint32_t tma_polls, uint32_t hold_tile);
+
 // Bytes of scratch memory (device) one sort of n keys of the given dtype needs:
 // the ping-pong key buffer, the per-sort state block and two look-back arrays.
 size_t radix_sort_temp_bytes(int dtype, size_t n);

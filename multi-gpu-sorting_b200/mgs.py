@@ -139,6 +139,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "mgs_tune_save": ([ctypes.c_char_p], c_int),
         "mgs_autotune": ([c_void, c_int, c_size, c_int, ctypes.POINTER(TuneSample), c_int, ctypes.POINTER(c_int)],
                          c_int),
+        "mgs_test_set_waits": ([c_int, c_u32, c_u32, c_u32], c_int),
+        "mgs_test_fail_device_allocations": ([c_int], c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -231,6 +233,21 @@ def sort_device_noalloc(d_keys: int, n: int, dtype, stream: int = 0) -> None:
     lib = load_library()
     _check(lib.mgs_sort_device_noalloc(dtype_code(dtype), ctypes.c_void_p(d_keys), int(n),
                                        ctypes.c_void_p(stream or None)))
+
+
+NO_HELD_TILE = 0xFFFFFFFF
+
+
+def inject_waits(device: int = 0, lookback_spins: int = 0, tma_polls: int = 0, hold_tile: int = NO_HELD_TILE):
+    """mgs_test_set_waits (failure injection for tests): bounds of the device-side waits (0 = default) and a
+    tile of the plain device sort whose look-back status is never published. Defaults restore normal sorts."""
+    _check(load_library().mgs_test_set_waits(int(device), int(lookback_spins), int(tma_polls), int(hold_tile)))
+
+
+def inject_allocation_failures(count: int) -> None:
+    """mgs_test_fail_device_allocations (failure injection for tests): the next `count` arena growths fail
+    with MGS_ERR_OOM."""
+    _check(load_library().mgs_test_fail_device_allocations(int(count)))
 
 
 class DataGenerator:

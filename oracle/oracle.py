@@ -227,3 +227,8 @@ def ref_cub_sort_range(dtype_code: int, d_keys: int, n: int, begin_bit: int, end
 
 def ref_num_procs() -> int:
     return ref_lib().ref_num_procs()
+
+
+def ref_phase_seconds(phase: str) -> float:
+    """The reference's TimeDurations entry `phase` (src/time_durations.cuh) of its last timed call, in seconds."""
+    return ref_lib().ref_phase_seconds(phase.encode())
