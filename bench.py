@@ -310,85 +310,100 @@ def small_batch_bench(mgs, torch, ctx, stream, reps=20):
             "graph_same_result": same}
 
 
-def served_bench(mgs, budget_s=2.0):
-    """Config 5b: Poisson arrivals at 10/50/90% of each form's measured peak, request sizes log-uniform over
-    2^10..2^26 keys, key type uniform over u32/i32/f32/u64; coalescing server against the plain form
-    (one request per launch, one slot). Requests come from a pool of pinned buffers that are submitted again
-    as they are once finished: every LSD radix pass and every in-shared-memory segment sort does the same
-    work on sorted keys, and refilling the buffers on the host (up to 512 MB a request) would measure the
-    host's memcpy instead of the engine. Results in the mix are checked byte for byte by the server tests."""
+def served_bench(mgs, torch, budget_s=2.0):
+    """Batched and served sorting, request stream: Poisson arrivals at 10/50/90% of the plain form's measured
+    peak (and the served form at 90% of its own), key type uniform over u32/i32/f32/u64, request keys resident
+    in HBM (mgs_server_submit_device, sorted in place). Two size mixes: log-uniform over 2^10..2^26 keys, and
+    small requests only (2^10..2^18). Forms: plain = one request per launch sequence, one at a time
+    (num_slots 1, no coalescing); served = continuous batching (4 batches in flight, requests up to 2^20 keys
+    coalesced, admission by free pool memory). Every request sorts fresh keys: once a request finishes, its
+    buffer is restored from a pristine device copy (outside its latency) before it is submitted again."""
     import threading
     import queue as _queue
-    rng = np.random.default_rng(7)
     types = ["u32", "i32", "f32", "u64"]
-    pool = []
-    for i, n in enumerate((2 ** rng.uniform(10, 26, 96)).astype(np.int64)):
-        a = mgs.generate(types[i % 4], "full-uniform", 100 + i, int(n))
-        h = mgs.host_empty(a.size, a.dtype)
-        h[:] = a
-        pool.append((a, h))
-    mean_keys = float(np.mean([a.size for a, _ in pool]))
+    out = {"arrivals": "Poisson", "types": types, "requests": "device-resident (mgs_server_submit_device)",
+           "offered_load": "fraction of the plain form's peak keys/s (served also at 0.9 of its own peak)",
+           "input": "each request's keys restored from a pristine device copy after it completes"}
+    for mix, (lo, hi) in (("log-uniform 2^10..2^26", (10, 26)), ("log-uniform 2^10..2^18", (10, 18))):
+        rng = np.random.default_rng(7)
+        pool = []
+        for i, n in enumerate((2 ** rng.uniform(lo, hi, 96)).astype(np.int64)):
+            dt = types[i % 4]
+            a = mgs.generate(dt, "full-uniform" + ("-specials" if dt == "f32" else ""), 100 + i, int(n))
+            st = np.int32 if a.dtype.itemsize == 4 else np.int64
+            pristine = torch.from_numpy(a.view(st)).cuda()
+            pool.append((dt, int(n), pristine, pristine.clone()))
+        torch.cuda.synchronize()
+        mean_keys = float(np.mean([p[1] for p in pool]))
+        restore_stream = torch.cuda.Stream()
 
-    def run(srv, rate, duration, max_requests):
-        free = _queue.Queue()
-        for i in range(len(pool)):
-            free.put(i)
-        done = _queue.Queue()
-
-        def reaper():
-            while True:
-                item = done.get()
-                if item is None:
-                    return
-                rid, i = item
-                assert srv.wait(rid) == mgs.MGS_OK
+        def run(srv, rate, duration, max_requests):
+            free = _queue.Queue()
+            for i in range(len(pool)):
                 free.put(i)
+            done = _queue.Queue()
 
-        th = threading.Thread(target=reaper)
-        th.start()
-        srv.stats(reset=True)
-        t0 = time.perf_counter()
-        nxt = t0
-        sent = 0
-        while sent < max_requests and time.perf_counter() - t0 < duration:
-            if rate is not None:
-                nxt += rng.exponential(1.0 / rate)
-                while time.perf_counter() < nxt:
-                    pass
-            i = free.get()
-            done.put((srv.submit(pool[i][1]), i))
-            sent += 1
-        done.put(None)
-        th.join()
-        st = srv.stats()
-        return {"requests": st["completed"], "keys_per_s": st["keys"] / max(st["busy_s"], 1e-9),
-                "p50_ms": st["p50_us"] / 1e3, "p99_ms": st["p99_us"] / 1e3, "batches": st["batches"]}
+            def reaper():
+                while True:
+                    item = done.get()
+                    if item is None:
+                        return
+                    rid, i = item
+                    assert srv.wait(rid) == mgs.MGS_OK
+                    with torch.cuda.stream(restore_stream):
+                        pool[i][3].copy_(pool[i][2])
+                    restore_stream.synchronize()
+                    free.put(i)
 
-    # Both forms see the same absolute arrival rates: 10, 50 and 90% of the plain form's peak; the served
-    # form also runs at 90% of its own peak.
-    out = {"request_keys": "log-uniform 2^10..2^26", "types": types, "pool": len(pool),
-           "offered_load": "fraction of the plain form's peak keys/s (served also at 0.9 of its own peak)"}
-    forms = [("plain", dict(num_slots=1, slot_keys=1 << 26, coalesce_keys=0)),
-             ("served", dict(num_slots=4, slot_keys=1 << 26, coalesce_keys=1 << 20))]
-    plain_peak = None
-    for name, cfg in forms:
-        srv = mgs.Server(0, **cfg)
-        try:
-            peak = run(srv, None, budget_s, 4 * len(pool))
-            if plain_peak is None:
-                plain_peak = peak["keys_per_s"]
-            levels = []
-            targets = [(load, load * plain_peak) for load in (0.1, 0.5, 0.9)]
-            if name == "served":
-                targets.append((round(0.9 * peak["keys_per_s"] / plain_peak, 3), 0.9 * peak["keys_per_s"]))
-            for load, keys_per_s in targets:
-                r = run(srv, keys_per_s / mean_keys, budget_s, 10_000)
-                r["offered_load"] = load
-                r["offered_keys_per_s"] = keys_per_s
-                levels.append(r)
-            out[name] = {"peak": peak, "loads": levels, "config": cfg}
-        finally:
-            srv.close()
+            th = threading.Thread(target=reaper)
+            th.start()
+            srv.stats(reset=True)
+            t0 = time.perf_counter()
+            nxt = t0
+            sent = 0
+            while sent < max_requests and time.perf_counter() - t0 < duration:
+                if rate is not None:
+                    nxt += rng.exponential(1.0 / rate)
+                    while time.perf_counter() < nxt:
+                        pass
+                i = free.get()
+                dt, n, _, work = pool[i]
+                done.put((srv.submit_device(work.data_ptr(), n, dt), i))
+                sent += 1
+            done.put(None)
+            th.join()
+            st = srv.stats()
+            return {"requests": st["completed"], "keys_per_s": st["keys"] / max(st["busy_s"], 1e-9),
+                    "p50_ms": st["p50_us"] / 1e3, "p99_ms": st["p99_us"] / 1e3, "batches": st["batches"],
+                    "kernel_launches": st["kernel_launches"]}
+
+        res = {"pool": len(pool), "mean_request_keys": mean_keys}
+        forms = [("plain", dict(num_slots=1, coalesce_keys=0)),
+                 ("served", dict(num_slots=4, coalesce_keys=1 << 20))]
+        plain_peak = None
+        for name, cfg in forms:
+            srv = mgs.Server(0, **cfg)
+            try:
+                run(srv, None, 0.5, 2 * len(pool))  # warm-up
+                peak = run(srv, None, budget_s, 8 * len(pool))
+                if plain_peak is None:
+                    plain_peak = peak["keys_per_s"]
+                levels = []
+                targets = [(load, load * plain_peak) for load in (0.1, 0.5, 0.9)]
+                if name == "served":
+                    targets.append((round(0.9 * peak["keys_per_s"] / plain_peak, 3), 0.9 * peak["keys_per_s"]))
+                for load, keys_per_s in targets:
+                    r = run(srv, keys_per_s / mean_keys, budget_s, 20_000)
+                    r["offered_load"] = load
+                    r["offered_keys_per_s"] = keys_per_s
+                    levels.append(r)
+                res[name] = {"peak": peak, "loads": levels, "config": cfg}
+            finally:
+                srv.close()
+        res["served_over_plain_peak"] = res["served"]["peak"]["keys_per_s"] / res["plain"]["peak"]["keys_per_s"]
+        out[mix] = res
+        del pool
+        torch.cuda.empty_cache()
     return out
 
 
@@ -978,7 +993,7 @@ def main():
             batched = {"u32": batched_bench(mgs, torch, ctx, "u32"),
                        "f32": batched_bench(mgs, torch, ctx, "f32", with_plain=False)}
         if not args.no_served:
-            served = served_bench(mgs)
+            served = served_bench(mgs, torch)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

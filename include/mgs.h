@@ -286,37 +286,47 @@ int mgs_ctx_phase_seconds(mgs_ctx* ctx, const char* phase, double* seconds);
 
 /* ---- serving loop (no counterpart in the reference) -------------------------
  * Sort requests of mixed sizes and key types, submitted from any thread, are
- * batched onto one GPU by a dispatcher thread (continuous batching): device
- * memory is reserved once as num_slots resident slots (as many as
- * device_budget_bytes admits); a queued request starts when a slot is free
- * (admission by free HBM); a small request (<= coalesce_keys) opens a batch
- * that every other queued small request of the same key type joins while the
- * slot has room, sorted by one segmented-sort launch sequence; larger requests
- * run alone. Each slot has its own stream, so batches overlap on the device.
- * Requests are sorted in place in the caller's host buffer (pinned for full
- * speed), which must stay valid until mgs_server_wait reports it finished.
- * coalesce_keys = 0 and num_slots = 1 give the plain one-request-per-launch
- * form. Zero config fields take defaults: num_slots 4, slot_keys 2^26 (keys of
- * up to 8 bytes per slot), coalesce_keys 0 (no coalescing), max_batch_requests
- * 4096, device_budget_bytes 80% of free device memory. */
+ * batched onto one GPU by a dispatcher thread (continuous batching).
+ *   Memory: one device pool of device_budget_bytes is reserved at creation
+ *   (0: half the free device memory, at most 32 GiB). Each batch takes exactly
+ *   the bytes it needs (staging keys, offsets, sort scratch) from the pool and
+ *   returns them when it finishes: a queued request is admitted when a stream
+ *   is free and the pool has room for it (admission by free HBM), in arrival
+ *   order. A request that would not fit even in the empty pool, or that has
+ *   more than slot_keys keys (0: no such limit), is refused at submission.
+ *   In flight: up to num_slots batches (default 4), each on its own stream.
+ *   Coalescing: a request of at most coalesce_keys keys (0: no coalescing)
+ *   opens a batch that queued small requests of a compatible key type join
+ *   (up to max_batch_requests, default 4096): uint32 with int32, uint64 with
+ *   int64 (signed keys sort as unsigned ones with the top bit inverted on the
+ *   way in and out), float32 and float64 each on their own; the batch is sorted
+ *   by one segmented-sort launch sequence. Larger requests run alone.
+ *   Requests: mgs_server_submit takes a host buffer (pinned for full speed),
+ *   mgs_server_submit_device a buffer in this GPU's memory, which a request
+ *   running alone sorts in place without any copy. Either is sorted in place
+ *   and must stay valid until mgs_server_wait reports it finished.
+ * num_slots = 1 with coalesce_keys = 0 gives the plain one-request-per-launch
+ * form. */
 typedef struct mgs_server mgs_server;
 typedef struct mgs_server_config {
   int device;
-  int num_slots;
-  size_t slot_keys;
-  size_t coalesce_keys;
-  size_t max_batch_requests;
-  size_t device_budget_bytes;
+  int num_slots;             /* batches in flight (streams) */
+  size_t slot_keys;          /* largest request in keys; 0 = limited by the pool only */
+  size_t coalesce_keys;      /* requests up to this many keys may share a batch; 0 = none */
+  size_t max_batch_requests; /* requests per coalesced batch */
+  size_t device_budget_bytes; /* device pool */
 } mgs_server_config;
 typedef struct mgs_server_stats {
   uint64_t submitted, completed, rejected, cancelled, batches, keys, kernel_launches;
   int num_slots;
   double p50_us, p99_us, mean_us, max_us; /* latency: completion - submission */
   double busy_s;                          /* first submission to last completion */
+  uint64_t pool_bytes, pool_free_bytes;   /* the device pool and its free bytes now */
 } mgs_server_stats;
 int mgs_server_create(const mgs_server_config* config, mgs_server** out);
 int mgs_server_destroy(mgs_server* server); /* finishes queued and running requests first */
 int mgs_server_submit(mgs_server* server, int dtype, void* h_keys, size_t n, uint64_t* request_id);
+int mgs_server_submit_device(mgs_server* server, int dtype, void* d_keys, size_t n, uint64_t* request_id);
 /* Waits for a request (timeout_ms < 0: no limit); MGS_ERR_TIMEOUT if it is still
  * running. *request_status: MGS_OK, MGS_ERR_CANCELLED or the failure. A request
  * is forgotten once a wait has reported it finished. */

@@ -35,6 +35,10 @@ struct KeyTraits {
     return b ^ (neg | kSign);
   }
   __host__ __device__ __forceinline__ static uint32_t Digit(BitsT b, int pass) {
+#ifdef __CUDA_ARCH__
+    // byte `pass` of a 4-byte key, zero-extended, in one byte-permute
+    if constexpr (sizeof(BitsT) == 4) return __byte_perm(uint32_t(Ordered(b)), 0u, 0x4440u | uint32_t(pass));
+#endif
     return uint32_t(Ordered(b) >> (pass * 8)) & 0xFFu;
   }
   // Strict "a before b" in radix order (equal keys are not before each other).

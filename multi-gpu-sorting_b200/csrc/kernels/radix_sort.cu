@@ -313,18 +313,35 @@ __device__ __forceinline__ uint32_t ballot_peers(uint32_t d, bool ok) {
 // that a short tile keeps every warp busy, and a warp stops at its first item
 // that lies wholly past `valid`. Without it the code is the fixed-span form
 // the onesweep kernel is tuned on.
+//
+// LEAN (the onesweep kernel's form) keeps the block barriers per tile at
+// three: the per-chain counters of a warp are zero on entry (each warp clears
+// its own rows after the tile's scatter), the first barrier also reduces
+// `arrived` (false on any thread: the tile's copy never completed; returns
+// kRankAborted before anything is written) and is followed by after_a() (the
+// next tile's copy may be issued into the other buffer from then on), and the
+// tile scan is a warp scan over the first eight warps plus one barrier.
+struct NoOp {
+  __device__ __forceinline__ void operator()() const {}
+};
+constexpr int kRankDone = 0, kRankSkipped = 1, kRankAborted = 2;
+
 template <class Tr, int BLOCK, int ITEMS, int CHAINS, int MATCH, bool FULL, bool ALLOW_SKIP, bool SPREAD = false,
-          typename V = NoValue, class OnCounts = void, class Between = void, class Dg = PlainDigits>
-__device__ __forceinline__ bool rank_tile(OnesweepSmem<Tr, BLOCK, ITEMS, CHAINS, V>& sm, const typename Tr::Bits* src,
-                                          typename Tr::Bits* dst, uint32_t valid, int pass, uint32_t* tile_count_out,
-                                          OnCounts on_counts, Between between, const V* src_val = nullptr,
-                                          V* dst_val = nullptr, Dg dg = Dg{}, uint32_t warp_items = ITEMS) {
+          bool LEAN = false, typename V = NoValue, class OnCounts = void, class Between = void,
+          class Dg = PlainDigits, class AfterA = NoOp>
+__device__ __forceinline__ int rank_tile(OnesweepSmem<Tr, BLOCK, ITEMS, CHAINS, V>& sm, const typename Tr::Bits* src,
+                                         typename Tr::Bits* dst, uint32_t valid, int pass, uint32_t* tile_count_out,
+                                         OnCounts on_counts, Between between, const V* src_val = nullptr,
+                                         V* dst_val = nullptr, Dg dg = Dg{}, uint32_t warp_items = ITEMS,
+                                         bool arrived = true, AfterA after_a = AfterA{}) {
   using Bits = typename Tr::Bits;
   constexpr int kTile = BLOCK * ITEMS;
   constexpr int kChains = (BLOCK / 32) * CHAINS;
   constexpr int kPerChain = ITEMS / CHAINS;
   static_assert(ITEMS % CHAINS == 0, "items split evenly into chains");
   static_assert(MATCH == 2 || MATCH == 3, "ranking modes: shared-memory masks, or half ballots");
+  static_assert(!(LEAN && ALLOW_SKIP), "the lean form has no identity-pass exit");
+  static_assert(BLOCK >= kRadix, "one thread per digit");
   const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
   constexpr bool kSpread = SPREAD && !FULL && CHAINS == 1;
@@ -333,8 +350,10 @@ __device__ __forceinline__ bool rank_tile(OnesweepSmem<Tr, BLOCK, ITEMS, CHAINS,
   // Warp-uniform: item i of this warp holds no key of the tile.
   auto item_done = [&](int i) { return kSpread && (i >= witems || uint32_t(wbase + i * 32) >= valid); };
 
-  for (int i = tid; i < kChains * kRadix; i += BLOCK) sm.ccount[i] = 0u;
-  __syncthreads();
+  if constexpr (!LEAN) {
+    for (int i = tid; i < kChains * kRadix; i += BLOCK) sm.ccount[i] = 0u;
+    __syncthreads();
+  }
   // Phase 1: per-chain digit counts.
   Bits key[ITEMS];
   V val[kHasValues<V> ? ITEMS : 1];
@@ -347,7 +366,12 @@ __device__ __forceinline__ bool rank_tile(OnesweepSmem<Tr, BLOCK, ITEMS, CHAINS,
     uint32_t* cc = sm.ccount + (warp * CHAINS + i / kPerChain) * kRadix;
     if (FULL || idx < valid) atomicAdd(&cc[dg.template digit<Tr>(key[i], pass)], 1u);
   }
-  __syncthreads();
+  if constexpr (LEAN) {
+    if (__syncthreads_or(!arrived)) return kRankAborted;
+    after_a();
+  } else {
+    __syncthreads();
+  }
 
   uint32_t tile_count = 0;
   if (tid < kRadix) {
@@ -357,10 +381,32 @@ __device__ __forceinline__ bool rank_tile(OnesweepSmem<Tr, BLOCK, ITEMS, CHAINS,
   }
   *tile_count_out = tile_count;
   if (ALLOW_SKIP) {
-    if (__syncthreads_or(tid < kRadix && tile_count == valid)) return true;
+    if (__syncthreads_or(tid < kRadix && tile_count == valid)) return kRankSkipped;
   }
-  uint32_t total;
-  const uint32_t tstart = block_exclusive_scan<BLOCK>(tid < kRadix ? tile_count : 0u, sm.scan_tmp, &total);
+  uint32_t tstart = 0;
+  if constexpr (LEAN) {
+    // exclusive scan of the 256 digit counts: a shuffle scan within each of the
+    // first eight warps, then the totals of the warps before.
+    uint32_t incl = tile_count;
+    if (tid < kRadix) {
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+      }
+      if (lane == 31) sm.scan_tmp[warp] = incl;
+    }
+    __syncthreads();
+    if (tid < kRadix) {
+      uint32_t before = 0;
+#pragma unroll
+      for (int w = 0; w < kRadix / 32; ++w) before += (w < warp) ? sm.scan_tmp[w] : 0u;
+      tstart = before + incl - tile_count;
+    }
+  } else {
+    uint32_t total;
+    tstart = block_exclusive_scan<BLOCK>(tid < kRadix ? tile_count : 0u, sm.scan_tmp, &total);
+  }
   if (tid < kRadix) {
     sm.tile_start[tid] = tstart;
     uint32_t run = tstart;
@@ -422,7 +468,7 @@ __device__ __forceinline__ bool rank_tile(OnesweepSmem<Tr, BLOCK, ITEMS, CHAINS,
       }
     }
   }
-  return false;
+  return kRankDone;
 }
 
 // Where one onesweep tile's keys come from and go to. For the plain sort the
@@ -450,13 +496,16 @@ struct ValueSpan {
 // values, svals being the tile's value buffer, when V is a value type).
 // SPREAD: a partial tile is ranked over all warps (ceil(valid / BLOCK) keys per
 // lane), as the segmented sort's many short last tiles want.
+// Returns true (block-uniform) when the tile's copy never completed; nothing
+// was written then. Otherwise the calling warp's counter rows are zero again on
+// return, and the tile's shared-memory buffer is no longer read.
 template <class Tr, int BLOCK, int ITEMS, int CHAINS, typename StatusT, int MATCH, bool FULL, bool SPREAD, typename V,
-          class Dg>
-__device__ __forceinline__ void onesweep_tile(OnesweepSmem<Tr, BLOCK, ITEMS, CHAINS, V>& sm, typename Tr::Bits* skeys,
+          class Dg, class AfterA>
+__device__ __forceinline__ bool onesweep_tile(OnesweepSmem<Tr, BLOCK, ITEMS, CHAINS, V>& sm, typename Tr::Bits* skeys,
                                               RadixState* __restrict__ st, StatusT* __restrict__ lb_cur,
                                               const TileSpan<Tr>& span, uint32_t tile, uint32_t valid, int pass,
                                               V* svals, const ValueSpan<V>& vspan, Dg dg, uint32_t spin_limit,
-                                              bool publish) {
+                                              bool publish, bool arrived, AfterA after_a) {
   using Bits = typename Tr::Bits;
   using LW = LookbackWord<StatusT>;
   const int tid = threadIdx.x;
@@ -468,7 +517,7 @@ __device__ __forceinline__ void onesweep_tile(OnesweepSmem<Tr, BLOCK, ITEMS, CHA
   // the waits on other tiles overlap ranking.
   uint32_t tile_count = 0;
   const uint32_t warp_items = (SPREAD && !FULL) ? (valid + BLOCK - 1) / BLOCK : uint32_t(ITEMS);
-  rank_tile<Tr, BLOCK, ITEMS, CHAINS, MATCH, FULL, false, SPREAD>(
+  const int ranked = rank_tile<Tr, BLOCK, ITEMS, CHAINS, MATCH, FULL, false, SPREAD, true>(
       sm, skeys, skeys, valid, pass, &tile_count,
       [&](uint32_t count) {
         StatusT* slot = lb_cur + size_t(tile) * kRadix + tid;
@@ -514,7 +563,8 @@ __device__ __forceinline__ void onesweep_tile(OnesweepSmem<Tr, BLOCK, ITEMS, CHA
         }
         sm.gbase[tid] = span.bucket[tid] + uint32_t(excl) - sm.tile_start[tid];
       },
-      svals, svals, dg, warp_items);
+      svals, svals, dg, warp_items, arrived, after_a);
+  if (ranked == kRankAborted) return true;
   __syncthreads();
 
   // Phase 3: consecutive threads write consecutive positions of one digit run.
@@ -531,6 +581,12 @@ __device__ __forceinline__ void onesweep_tile(OnesweepSmem<Tr, BLOCK, ITEMS, CHA
       }
     }
   }
+  // This warp's counter rows back to zero for the next tile: no other warp
+  // touches them before the next tile's first barrier.
+  uint32_t* own = sm.ccount + (tid >> 5) * CHAINS * kRadix;
+  for (int j = tid & 31; j < CHAINS * kRadix; j += 32) own[j] = 0u;
+  __syncwarp();
+  return false;
 }
 
 // Large segments of a segmented sort, as seen by the onesweep kernels.
@@ -653,18 +709,22 @@ __global__ __launch_bounds__(BLOCK, MINB) void radix_onesweep_kernel(typename Tr
     if constexpr (kHasValues<V>) bulk_copy_g2s(sm.vals.v[b], w.v.start, w.v.bytes, &sm.bar[b]);
   };
 
-  // Persistent CTA: tiles come in launch order from an atomic counter; the
-  // next tile is claimed and its TMA bulk copy issued before the current tile
-  // is ranked, so loads overlap compute. A CTA's current tile is always older
-  // than its prefetched one, so the oldest unfinished tile is always being
-  // processed and the look-back makes progress.
+  // Persistent CTA: tiles come in launch order from an atomic counter. The
+  // next tile is claimed (and its span worked out) at the top of each
+  // iteration, and its TMA bulk copy is issued into the other buffer as soon
+  // as every warp is past the current tile's first barrier (that buffer's
+  // previous tile is then fully scattered), so loads overlap ranking. A CTA's
+  // current tile is always older than its prefetched one, so the oldest
+  // unfinished tile is always being processed and the look-back makes
+  // progress.
   static_assert(sizeof(TileSpan<Tr>) <= sizeof(sm.span[0]), "span slot");
   TileSpan<Tr>* spans = reinterpret_cast<TileSpan<Tr>*>(sm.span);
   for (int i = tid; i < kChains * 2 * kRadix; i += BLOCK) sm.masks[i] = 0u;
-  // The thread that claims tiles and issues their copies. A segment's tile
-  // span takes a few dependent loads; in the segmented sort a thread of the
-  // last warp does it, as the first warps also run the look-back.
-  constexpr int kLeader = SEG ? BLOCK - 32 : 0;
+  for (int i = tid; i < kChains * kRadix; i += BLOCK) sm.ccount[i] = 0u;  // then kept zero by each warp
+  // The thread that claims tiles and issues their copies: a thread of the last
+  // warp (the first eight warps run the tile scan and the look-back; a
+  // segment's tile span takes a few dependent loads).
+  constexpr int kLeader = BLOCK - 32;
   if (tid == kLeader) {
     mbar_init(&sm.bar[0], 1);
     mbar_init(&sm.bar[1], 1);
@@ -684,19 +744,24 @@ __global__ __launch_bounds__(BLOCK, MINB) void radix_onesweep_kernel(typename Tr
   for (;;) {
     const uint32_t tile = sm.tile_id[cur];
     if (tile >= num_tiles) break;
+    // Every thread read tile_id / spans of the other slot one iteration ago.
+    uint32_t next_tile = num_tiles;
+    Windows next_win{};
     if (tid == kLeader) {
-      const uint32_t t = atomicAdd(&st->tile_counter[pass], 1u);
-      sm.tile_id[cur ^ 1] = t;
-      if (t < num_tiles) {
-        const TileSpan<Tr> sp = span_of(t);
+      next_tile = atomicAdd(&st->tile_counter[pass], 1u);
+      sm.tile_id[cur ^ 1] = next_tile;
+      if (next_tile < num_tiles) {
+        const TileSpan<Tr> sp = span_of(next_tile);
         spans[cur ^ 1] = sp;
-        const Windows w = windows_of(sp, t);
-        if (w.tma) {
-          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-          issue_copy(cur ^ 1, w);
-        }
+        next_win = windows_of(sp, next_tile);
       }
     }
+    auto issue_next = [&] {
+      if (tid == kLeader && next_tile < num_tiles && next_win.tma) {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        issue_copy(cur ^ 1, next_win);
+      }
+    };
     const TileSpan<Tr> span = spans[cur];
     const size_t base = size_t(tile - span.first_tile) * kTile;
     const uint32_t valid = uint32_t(min(size_t(kTile), size_t(span.seg_len) - base));
@@ -704,33 +769,36 @@ __global__ __launch_bounds__(BLOCK, MINB) void radix_onesweep_kernel(typename Tr
     Bits* skeys = sm.keys[cur];
     V* svals = nullptr;
     if constexpr (kHasValues<V>) svals = sm.vals.v[cur];
+    bool arrived = true;
     if (win.tma) {
-      const bool arrived = mbar_wait_bounded(&sm.bar[cur], (parity >> cur) & 1u, wc.tma_polls);
+      // (the first barrier of the tile reduces `arrived`: a block-uniform exit when the copy never completed)
+      arrived = mbar_wait_bounded(&sm.bar[cur], (parity >> cur) & 1u, wc.tma_polls);
       parity ^= 1u << cur;
-      if (__syncthreads_or(!arrived)) {  // block-uniform exit when the copy never completed
-        if (tid == 0) atomicOr(&st->error, kStatusTmaTimeout);
-        return;
-      }
       skeys += win.k.shift;
       if constexpr (kHasValues<V>) svals += win.v.shift;
     } else {
       for (uint32_t i = tid; i < valid; i += BLOCK) skeys[i] = span.src[base + i];
       if constexpr (kHasValues<V>)
         for (uint32_t i = tid; i < valid; i += BLOCK) svals[i] = vspan.src[size_t(span.src - src) + base + i];
+      __syncthreads();
     }
+    bool aborted;
     if (valid == uint32_t(kTile)) {
-      onesweep_tile<Tr, BLOCK, ITEMS, CHAINS, StatusT, MATCH, true, false>(sm, skeys, st, lb_cur, span, tile, valid,
-                                                                           pass, svals, vspan, dg, wc.lookback_spins,
-                                                                           tile != held);
+      aborted = onesweep_tile<Tr, BLOCK, ITEMS, CHAINS, StatusT, MATCH, true, false>(
+          sm, skeys, st, lb_cur, span, tile, valid, pass, svals, vspan, dg, wc.lookback_spins, tile != held, arrived,
+          issue_next);
     } else {
       // Partial tiles are spread over all warps in the segmented sort only: the
       // plain sort has one partial tile per pass, and its kernel keeps the
       // fixed-span code it is tuned on.
-      onesweep_tile<Tr, BLOCK, ITEMS, CHAINS, StatusT, MATCH, false, SEG>(sm, skeys, st, lb_cur, span, tile, valid,
-                                                                          pass, svals, vspan, dg, wc.lookback_spins,
-                                                                          tile != held);
+      aborted = onesweep_tile<Tr, BLOCK, ITEMS, CHAINS, StatusT, MATCH, false, SEG>(
+          sm, skeys, st, lb_cur, span, tile, valid, pass, svals, vspan, dg, wc.lookback_spins, tile != held, arrived,
+          issue_next);
     }
-    __syncthreads();
+    if (aborted) {
+      if (tid == 0) atomicOr(&st->error, kStatusTmaTimeout);
+      return;
+    }
     cur ^= 1;
   }
 }

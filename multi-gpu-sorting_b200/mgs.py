@@ -60,7 +60,7 @@ class ServerStats(ctypes.Structure):
                 ("cancelled", ctypes.c_uint64), ("batches", ctypes.c_uint64), ("keys", ctypes.c_uint64),
                 ("kernel_launches", ctypes.c_uint64), ("num_slots", ctypes.c_int), ("p50_us", ctypes.c_double),
                 ("p99_us", ctypes.c_double), ("mean_us", ctypes.c_double), ("max_us", ctypes.c_double),
-                ("busy_s", ctypes.c_double)]
+                ("busy_s", ctypes.c_double), ("pool_bytes", ctypes.c_uint64), ("pool_free_bytes", ctypes.c_uint64)]
 
 
 class TuneSample(ctypes.Structure):
@@ -122,6 +122,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "mgs_server_create": ([ctypes.POINTER(ServerConfig), ctypes.POINTER(c_void)], c_int),
         "mgs_server_destroy": ([c_void], c_int),
         "mgs_server_submit": ([c_void, c_int, c_void, c_size, ctypes.POINTER(ctypes.c_uint64)], c_int),
+        "mgs_server_submit_device": ([c_void, c_int, c_void, c_size, ctypes.POINTER(ctypes.c_uint64)], c_int),
         "mgs_server_wait": ([c_void, ctypes.c_uint64, c_int, ctypes.POINTER(c_int)], c_int),
         "mgs_server_cancel": ([c_void, ctypes.c_uint64], c_int),
         "mgs_server_stats_get": ([c_void, ctypes.POINTER(ServerStats), c_int], c_int),
@@ -518,6 +519,15 @@ class Server:
         _check(self._lib.mgs_server_submit(self.handle, dtype_code(keys.dtype), keys.ctypes.data_as(ctypes.c_void_p),
                                            keys.size, ctypes.byref(rid)))
         self._keep[rid.value] = keys
+        return rid.value
+
+    def submit_device(self, d_keys: int, n: int, dtype, keep=None) -> int:
+        """Queues n keys of `dtype` at device address d_keys (this server's GPU), sorted in place; returns the
+        request id. The buffer must stay valid until wait(); `keep` is held until then (e.g. the tensor)."""
+        rid = ctypes.c_uint64()
+        _check(self._lib.mgs_server_submit_device(self.handle, dtype_code(dtype), ctypes.c_void_p(d_keys), int(n),
+                                                  ctypes.byref(rid)))
+        self._keep[rid.value] = keep
         return rid.value
 
     def wait(self, request_id: int, timeout_ms: int = -1) -> int:

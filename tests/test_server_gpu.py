@@ -109,3 +109,113 @@ def test_limits_cancel_and_timeout(mgs):
         assert srv.stats()["cancelled"] == cancelled
     finally:
         srv.close()
+
+
+torch = pytest.importorskip("torch")
+DEVICE_TYPES = ["u32", "i32", "f32", "u64", "i64", "f64"]
+
+
+def device_requests(mgs, seed, count, max_log2=17):
+    """(input copy on the host, device tensor holding the same keys) per request: mixed types and sizes."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        dtype = DEVICE_TYPES[rng.integers(0, len(DEVICE_TYPES))]
+        n = int(2 ** rng.uniform(0, max_log2))
+        dist = "full-uniform-specials" if dtype in ("f32", "f64") else "full-uniform"
+        a = mgs.generate(dtype, dist, seed * 1000 + i, n)
+        st = np.int32 if a.dtype.itemsize == 4 else np.int64
+        out.append((a, torch.from_numpy(a.view(st).copy()).cuda()))
+    torch.cuda.synchronize()
+    return out
+
+
+def test_device_requests_match_oracle_alone_and_in_mix(mgs, orc):
+    reqs = device_requests(mgs, 21, 240)
+    srv = mgs.Server(0, num_slots=4, coalesce_keys=1 << 14)
+    try:
+        ids = [srv.submit_device(t.data_ptr(), a.size, a.dtype, keep=t) for a, t in reqs]
+        assert all(srv.wait(i) == mgs.MGS_OK for i in ids)
+        mixed = [t.cpu().numpy().view(a.dtype) for a, t in reqs]
+        for (a, _), got in zip(reqs, mixed):
+            assert got.tobytes() == orc.sort(a).tobytes()
+        assert srv.stats()["batches"] < len(reqs)
+        # alone, one at a time, each request gives the same bytes as in the mix
+        for (a, _), got in list(zip(reqs, mixed))[:60]:
+            st = np.int32 if a.dtype.itemsize == 4 else np.int64
+            t = torch.from_numpy(a.view(st).copy()).cuda()
+            torch.cuda.synchronize()
+            assert srv.wait(srv.submit_device(t.data_ptr(), a.size, a.dtype, keep=t)) == mgs.MGS_OK
+            assert t.cpu().numpy().view(a.dtype).tobytes() == got.tobytes()
+    finally:
+        srv.close()
+
+
+def test_uint32_and_int32_requests_share_one_batch(mgs, orc):
+    """Small uint32 and int32 requests are sorted by one segmented launch: the int32 keys with their top bit
+    inverted on the way in and out, which must still give int32 order."""
+    reqs = []
+    for i in range(64):
+        dtype = "i32" if i % 2 else "u32"
+        a = mgs.generate(dtype, "full-uniform", 500 + i, 1000 + 37 * i)
+        h = mgs.host_empty(a.size, a.dtype)
+        h[:] = a
+        reqs.append((a, h))
+    srv = mgs.Server(0, num_slots=1, coalesce_keys=1 << 16)
+    try:
+        blocker = mgs.host_empty(1 << 24, np.uint32)  # keeps the only stream busy while the small ones queue
+        blocker[:] = mgs.generate("u32", "full-uniform", 1, blocker.size)
+        first = srv.submit(blocker)
+        ids = [srv.submit(h) for _, h in reqs]
+        assert srv.wait(first) == mgs.MGS_OK
+        assert all(srv.wait(i) == mgs.MGS_OK for i in ids)
+        for a, h in reqs:
+            assert h.tobytes() == orc.sort(a).tobytes()
+        assert srv.stats()["batches"] <= 3  # the blocker, then the queued small requests together
+    finally:
+        srv.close()
+
+
+def test_mixed_host_and_device_requests_in_one_batch(mgs, orc):
+    reqs_h = make_requests(mgs, 31, 30, max_log2=12)
+    reqs_d = device_requests(mgs, 32, 30, max_log2=12)
+    srv = mgs.Server(0, num_slots=1, coalesce_keys=1 << 12)
+    try:
+        ids = []
+        for (ah, h), (ad, t) in zip(reqs_h, reqs_d):
+            ids.append(srv.submit(h))
+            ids.append(srv.submit_device(t.data_ptr(), ad.size, ad.dtype, keep=t))
+        assert all(srv.wait(i) == mgs.MGS_OK for i in ids)
+        for a, h in reqs_h:
+            assert h.tobytes() == orc.sort(a).tobytes()
+        for a, t in reqs_d:
+            assert t.cpu().numpy().view(a.dtype).tobytes() == orc.sort(a).tobytes()
+    finally:
+        srv.close()
+
+
+def test_admission_by_free_pool_memory(mgs, orc):
+    """A small pool: requests queue until earlier batches give their bytes back; one that could never fit is
+    refused at submission; the pool is whole again when everything is done."""
+    pool = 96 << 20
+    srv = mgs.Server(0, num_slots=4, coalesce_keys=0, device_budget_bytes=pool)
+    try:
+        n = 3 << 20  # ~12 MB of keys + ~13 MB of scratch as a host request: three fit at a time
+        reqs = []
+        for i in range(12):
+            a = mgs.generate("u32", "full-uniform", 700 + i, n)
+            h = mgs.host_empty(n, np.uint32)
+            h[:] = a
+            reqs.append((a, h))
+        ids = [srv.submit(h) for _, h in reqs]
+        assert all(srv.wait(i) == mgs.MGS_OK for i in ids)
+        for a, h in reqs:
+            assert h.tobytes() == orc.sort(a).tobytes()
+        huge = mgs.host_empty(16 << 20, np.uint64)
+        with pytest.raises(mgs.MgsError) as e:
+            srv.submit(huge)
+        assert e.value.code == mgs.MGS_ERR_INVALID
+        st = srv.stats()
+        assert st["pool_bytes"] == pool and st["pool_free_bytes"] == pool and st["rejected"] == 1
+    finally:
+        srv.close()
