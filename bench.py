@@ -316,8 +316,10 @@ def served_bench(mgs, torch, budget_s=2.0):
     in HBM (mgs_server_submit_device, sorted in place). Two size mixes: log-uniform over 2^10..2^26 keys, and
     small requests only (2^10..2^18). Forms: plain = one request per launch sequence, one at a time
     (num_slots 1, no coalescing); served = continuous batching (4 batches in flight, requests up to 2^20 keys
-    coalesced, admission by free pool memory). Every request sorts fresh keys: once a request finishes, its
-    buffer is restored from a pristine device copy (outside its latency) before it is submitted again."""
+    coalesced, admission by free pool memory). Peak: the whole pool of 96 requests submitted at once (a full
+    queue), four rounds, keys over the server's busy time. Every request sorts fresh keys: once a request
+    finishes, its buffer is restored from a pristine device copy (outside its latency) before it is submitted
+    again."""
     import threading
     import queue as _queue
     types = ["u32", "i32", "f32", "u64"]
@@ -337,23 +339,65 @@ def served_bench(mgs, torch, budget_s=2.0):
         mean_keys = float(np.mean([p[1] for p in pool]))
         restore_stream = torch.cuda.Stream()
 
+        def restore(idx):
+            with torch.cuda.stream(restore_stream):
+                torch._foreach_copy_([pool[i][3] for i in idx], [pool[i][2] for i in idx])
+            restore_stream.synchronize()
+
+        def summary(st):
+            return {"requests": st["completed"], "keys_per_s": st["keys"] / max(st["busy_s"], 1e-9),
+                    "p50_ms": st["p50_us"] / 1e3, "p99_ms": st["p99_us"] / 1e3, "batches": st["batches"],
+                    "kernel_launches": st["kernel_launches"]}
+
+        def burst(srv, rounds):
+            """The whole pool submitted at once, `rounds` times (inputs restored between rounds, outside the
+            server's busy time): the server's throughput with a full queue."""
+            keys = busy = 0.0
+            lat = []
+            batches = launches = 0
+            for _ in range(rounds):
+                restore(range(len(pool)))
+                srv.stats(reset=True)
+                ids = [srv.submit_device(w.data_ptr(), n, dt) for dt, n, _, w in pool]
+                assert all(srv.wait(i) == mgs.MGS_OK for i in ids)
+                st = srv.stats()
+                keys += st["keys"]
+                busy += st["busy_s"]
+                lat += [st["p50_us"], st["p99_us"]]
+                batches += st["batches"]
+                launches += st["kernel_launches"]
+            restore(range(len(pool)))
+            return {"requests": rounds * len(pool), "keys_per_s": keys / max(busy, 1e-9), "rounds": rounds,
+                    "p50_ms_median_round": statistics.median(lat[0::2]) / 1e3,
+                    "p99_ms_median_round": statistics.median(lat[1::2]) / 1e3, "batches": batches,
+                    "kernel_launches": launches}
+
         def run(srv, rate, duration, max_requests):
+            """Poisson arrivals at `rate` requests/s; a finished request's buffer is restored (in groups, on a
+            side stream) before it is submitted again."""
             free = _queue.Queue()
             for i in range(len(pool)):
                 free.put(i)
             done = _queue.Queue()
 
             def reaper():
-                while True:
-                    item = done.get()
-                    if item is None:
-                        return
-                    rid, i = item
-                    assert srv.wait(rid) == mgs.MGS_OK
-                    with torch.cuda.stream(restore_stream):
-                        pool[i][3].copy_(pool[i][2])
-                    restore_stream.synchronize()
-                    free.put(i)
+                stop = False
+                while not stop:
+                    items = [done.get()]
+                    while True:
+                        try:
+                            items.append(done.get_nowait())
+                        except _queue.Empty:
+                            break
+                    if items[-1] is None:
+                        stop = True
+                        items.pop()
+                    for rid, _ in items:
+                        assert srv.wait(rid) == mgs.MGS_OK
+                    if items:
+                        restore([i for _, i in items])
+                        for _, i in items:
+                            free.put(i)
 
             th = threading.Thread(target=reaper)
             th.start()
@@ -362,20 +406,16 @@ def served_bench(mgs, torch, budget_s=2.0):
             nxt = t0
             sent = 0
             while sent < max_requests and time.perf_counter() - t0 < duration:
-                if rate is not None:
-                    nxt += rng.exponential(1.0 / rate)
-                    while time.perf_counter() < nxt:
-                        pass
+                nxt += rng.exponential(1.0 / rate)
+                while time.perf_counter() < nxt:
+                    pass
                 i = free.get()
                 dt, n, _, work = pool[i]
                 done.put((srv.submit_device(work.data_ptr(), n, dt), i))
                 sent += 1
             done.put(None)
             th.join()
-            st = srv.stats()
-            return {"requests": st["completed"], "keys_per_s": st["keys"] / max(st["busy_s"], 1e-9),
-                    "p50_ms": st["p50_us"] / 1e3, "p99_ms": st["p99_us"] / 1e3, "batches": st["batches"],
-                    "kernel_launches": st["kernel_launches"]}
+            return summary(srv.stats())
 
         res = {"pool": len(pool), "mean_request_keys": mean_keys}
         forms = [("plain", dict(num_slots=1, coalesce_keys=0)),
@@ -384,8 +424,8 @@ def served_bench(mgs, torch, budget_s=2.0):
         for name, cfg in forms:
             srv = mgs.Server(0, **cfg)
             try:
-                run(srv, None, 0.5, 2 * len(pool))  # warm-up
-                peak = run(srv, None, budget_s, 8 * len(pool))
+                burst(srv, 1)  # warm-up
+                peak = burst(srv, 4)
                 if plain_peak is None:
                     plain_peak = peak["keys_per_s"]
                 levels = []

@@ -442,6 +442,26 @@ int mgs_sort_range_device(mgs_ctx* ctx, int dtype, void* d_keys, void* d_values,
   return MGS_OK;
 }
 
+namespace {
+// Phases of one TanasicSort-style call, named like the reference's TimeDurations
+// keys (src/tanasic_sort.cuh:229-298): memory_allocation = time spent growing
+// the context arena in this call (0 once it is large enough), sort_phase = the
+// rest of the call (copies, sorts and merges); the arena is kept, so there is
+// no deallocation phase.
+struct CallPhases {
+  Context& c;
+  std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+  explicit CallPhases(Context& ctx) : c(ctx) { c.reserve_s = 0; }
+  ~CallPhases() {
+    const double total = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    c.phase_s[0] = c.reserve_s;
+    c.phase_s[1] = total > c.reserve_s ? total - c.reserve_s : 0.0;
+    c.phase_s[2] = 0;
+    c.phase_s[3] = 0;
+  }
+};
+}  // namespace
+
 int mgs_sort_host(mgs_ctx* ctx, int dtype, void* h_keys, size_t n) {
   if (!ctx) return invalid("mgs_sort_host: ctx is null");
   const size_t w = mgs::dtype_bytes(dtype);
@@ -451,6 +471,7 @@ int mgs_sort_host(mgs_ctx* ctx, int dtype, void* h_keys, size_t n) {
   if (n > kMaxDeviceSortKeys) return invalid("mgs_sort_host: n must be below 2^32");
   Context& c = ctx->impl;
   DeviceGuard g(c.device);
+  CallPhases phases(c);
   if (mgs::plan_staged(n, w).slabs > 1) {
     // Copies overlapped with slab sorts and a windowed merge; needs room for
     // two copies of the keys, else the plain path below runs.
@@ -511,6 +532,7 @@ int mgs_tanasic_sort(mgs_ctx* ctx, int dtype, void* h_keys, size_t n, int num_ch
   if (num_chunks == 1) return mgs_sort_host(ctx, dtype, h_keys, n);
   Context& c = ctx->impl;
   DeviceGuard g(c.device);
+  CallPhases phases(c);
   const mgs::ChunkPlan plan = mgs::plan_chunks(n, num_chunks);
   if (plan.chunk > kMaxDeviceSortKeys) return invalid("mgs_tanasic_sort: chunks must hold fewer than 2^32 keys");
   const size_t temp = mgs::chunk_sort_temp_bytes(dtype, n, num_chunks);

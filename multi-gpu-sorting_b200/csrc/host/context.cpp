@@ -1,6 +1,7 @@
 #include "context.h"
 
 #include <atomic>
+#include <chrono>
 #include <cstdio>
 #include <cstring>
 
@@ -84,6 +85,12 @@ cudaError_t Context::reserve(size_t bytes) {
   for (int left = g_failing_reservations.load(); left > 0;) {
     if (g_failing_reservations.compare_exchange_weak(left, left - 1)) return cudaErrorMemoryAllocation;
   }
+  const auto t0 = std::chrono::steady_clock::now();
+  struct Timed {
+    double& acc;
+    std::chrono::steady_clock::time_point t0;
+    ~Timed() { acc += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); }
+  } timed{reserve_s, t0};
   cudaError_t e = cudaDeviceSynchronize();
   if (e != cudaSuccess) return e;
   if (arena) cudaFree(arena);

@@ -65,6 +65,7 @@ struct Context {
   void* host_arena = nullptr;  // grow-only pinned host buffer (out-of-core sorted runs)
   size_t host_arena_bytes = 0;
   double phase_s[4] = {0, 0, 0, 0};  // last call's memory_allocation, sort_phase, merge_phase, memory_deallocation
+  double reserve_s = 0;              // seconds spent growing the arena since the counter was last reset
 
   // Ensures the pinned host arena holds at least `bytes`.
   cudaError_t reserve_host(size_t bytes);

@@ -12,7 +12,10 @@
 //   request is never starved by small ones). A request that could not fit even
 //   in the empty pool is refused at submission.
 // * Up to num_slots batches are in flight, each on its own stream, so batches
-//   overlap on the device (one batch's copies with another's kernels).
+//   overlap on the device (one batch's copies with another's kernels). At most
+//   one of them is large enough to fill the GPU by itself; while one runs, a
+//   queued large request waits and the small requests behind it may start
+//   (the large one is next as soon as the running one finishes).
 // * Coalescing: a request of at most coalesce_keys keys opens a batch that
 //   every other queued small request of a compatible key type joins (FIFO
 //   order) while the pool has room: uint32 with int32, uint64 with int64
@@ -52,6 +55,10 @@ using Clock = std::chrono::steady_clock;
 
 constexpr size_t kAlign = 256;
 inline size_t align_up(size_t x) { return (x + kAlign - 1) / kAlign * kAlign; }
+// A batch of at least this many keys keeps every SM busy on its own (hundreds
+// of onesweep tiles per pass): two of them at once only take SMs from each
+// other, so at most one such batch is in flight; smaller batches run beside it.
+constexpr size_t kLargeBatchKeys = size_t(1) << 22;
 
 struct Request {
   uint64_t id = 0;
@@ -319,12 +326,25 @@ struct Server {
   }
 
   // Forms the next batch from the queue for a free lane (lock held): the oldest
-  // request, plus compatible small ones while the pool has room. Returns null
-  // when the queue is empty or the oldest request does not fit yet.
+  // request that may start (the oldest of all unless it is large while a large
+  // batch runs; then the oldest small one), plus compatible small ones while
+  // the pool has room. Returns null when nothing may start, or when the chosen
+  // request does not fit in the pool yet.
   std::unique_ptr<Batch> form_batch() {
     while (!queue.empty() && queue.front()->state == Request::kCancelled) queue.pop_front();
     if (queue.empty()) return nullptr;
-    const auto head = queue.front();
+    const bool large_running = std::any_of(lanes.begin(), lanes.end(), [](const Lane& l) {
+      return l.batch && l.batch->total >= kLargeBatchKeys;
+    });
+    std::shared_ptr<Request> head;
+    for (const auto& r : queue) {
+      if (r->state != Request::kQueued) continue;
+      if (r->n < kLargeBatchKeys || !large_running) {
+        head = r;
+        break;
+      }
+    }
+    if (!head) return nullptr;
     auto b = std::make_unique<Batch>();
     b->reqs.assign(1, head);
     b->sort_dtype = head->dtype;
@@ -335,9 +355,11 @@ struct Server {
     if (b->layout.total > room) return nullptr;  // wait for retirements
     if (head->n <= cfg.coalesce_keys) {
       const int group = batch_group(head->dtype);
-      for (auto it = std::next(queue.begin()); it != queue.end() && b->reqs.size() < cfg.max_batch_requests; ++it) {
+      for (auto it = queue.begin(); it != queue.end() && b->reqs.size() < cfg.max_batch_requests; ++it) {
         const auto& r = *it;
-        if (r->state != Request::kQueued || batch_group(r->dtype) != group || r->n > cfg.coalesce_keys) continue;
+        if (r == head || r->state != Request::kQueued || batch_group(r->dtype) != group || r->n > cfg.coalesce_keys)
+          continue;
+        if (large_running && b->total + r->n >= kLargeBatchKeys) continue;  // stays a small batch
         const BatchLayout L = batch_layout(group, b->total + r->n, b->reqs.size() + 1, any_host || !r->on_device);
         if (L.total > room) break;
         b->reqs.push_back(r);

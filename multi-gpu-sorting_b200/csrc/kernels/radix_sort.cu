@@ -273,15 +273,23 @@ __device__ __forceinline__ constexpr bool rank_by_ballot(int h, int j) {
   return MATCH == 3 && (CHAINS == 1 ? (j & 1) == 0 : h == 0);
 }
 
+// The peer mask from 8 ballots, one per digit bit: lane k (and k + 16) forms
+// the masks of the lanes whose low / high nibble equals k & 15 (four ballots
+// each, with k's bits as lane constants), and every lane fetches the two masks
+// of its own nibbles with two shuffles: fewer integer operations per item than
+// combining all eight ballots in every lane.
 template <bool FULL>
 __device__ __forceinline__ uint32_t ballot_peers(uint32_t d, bool ok) {
-  uint32_t peers = 0xffffffffu;
+  const uint32_t k = threadIdx.x & 15u;
+  uint32_t mlo = 0xffffffffu, mhi = 0xffffffffu;
 #pragma unroll
-  for (int b = 0; b < 8; ++b) {
-    const bool bit = (d >> b) & 1u;
-    const uint32_t bal = __ballot_sync(0xffffffffu, bit);
-    peers &= bit ? bal : ~bal;
+  for (int b = 0; b < 4; ++b) {
+    const uint32_t kb = ((k >> b) & 1u) - 1u;  // 0 where k has bit b, all ones where it has not
+    mlo &= __ballot_sync(0xffffffffu, (d >> b) & 1u) ^ kb;
+    mhi &= __ballot_sync(0xffffffffu, (d >> (b + 4)) & 1u) ^ kb;
   }
+  uint32_t peers =
+      __shfl_sync(0xffffffffu, mlo, int(d & 15u)) & __shfl_sync(0xffffffffu, mhi, int((d >> 4) & 15u));
   if (!FULL) {
     const uint32_t bal = __ballot_sync(0xffffffffu, ok);
     peers &= ok ? bal : ~bal;
@@ -368,10 +376,10 @@ __device__ __forceinline__ int rank_tile(OnesweepSmem<Tr, BLOCK, ITEMS, CHAINS, 
   }
   if constexpr (LEAN) {
     if (__syncthreads_or(!arrived)) return kRankAborted;
-    after_a();
   } else {
     __syncthreads();
   }
+  after_a();
 
   uint32_t tile_count = 0;
   if (tid < kRadix) {
