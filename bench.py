@@ -674,6 +674,51 @@ def sweep_merge(mgs, torch, n, reps=3):
     ctx.close()
 
 
+def sweep_range(mgs, torch, n=1 << 30, reps=3):
+    """Descending order and bit ranges (CUB's SortKeysDescending / begin_bit, end_bit forms) on 2^30 device-
+    resident u32 keys: descending over all 32 bits, and ascending / descending by bits [8, 24). Checked on the
+    device against torch's stable sort of the same bit field. Algorithmic bytes: 2 x 4 B per pass that the range
+    needs plus one histogram read."""
+    ctx = mgs.Context(0)
+    peak, _ = measured_hbm_peak()
+    stream = torch.cuda.Stream()
+    src = torch.empty(n, dtype=torch.int32, device="cuda")
+    ctx.generate_device(src.data_ptr(), n, "u32", "full-uniform", SEED)
+    work = torch.empty_like(src)
+    temp_bytes = mgs.Context.sort_temp_bytes("u32", n)
+    temp = torch.empty(temp_bytes, dtype=torch.uint8, device="cuda")
+    for begin, end, desc in ((0, 32, True), (8, 24, False), (8, 24, True)):
+        times = []
+        for i in range(reps + 1):
+            with torch.cuda.stream(stream):
+                work.copy_(src)
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                ctx.sort_range_device(work.data_ptr(), n, "u32", begin, end, desc, d_temp=temp.data_ptr(),
+                                      temp_bytes=temp_bytes, stream=stream.cuda_stream)
+                b.record(stream)
+            stream.synchronize()
+            if i > 0:
+                times.append(a.elapsed_time(b))
+        ctx.synchronize()
+        field = ((src.to(torch.int64) & 0xFFFFFFFF) >> begin) & ((1 << (end - begin)) - 1)
+        if desc:
+            field = ((1 << (end - begin)) - 1) - field
+        idx = torch.sort(field, stable=True)[1]
+        del field
+        ok = bool(torch.equal(src[idx], work))
+        del idx
+        torch.cuda.empty_cache()
+        ms = statistics.median(times)
+        passes = (end - begin + 7) // 8
+        alg = n * 4 * (2 * passes + 1)
+        print(json.dumps({"sweep": "range", "dtype": "u32", "n": n, "begin_bit": begin, "end_bit": end,
+                          "descending": desc, "ms": ms, "keys_per_s": n / (ms / 1e3),
+                          "hbm_alg_gbs": alg / (ms / 1e3) / 1e9, "roofline_frac": alg / (ms / 1e3) / 1e9 / peak,
+                          "reps": reps, "verified": ok}), flush=True)
+    ctx.close()
+
+
 def sweep_pairs(mgs, torch, n32=1 << 30, reps=3):
     """Key-value sort (thrust::sort_by_key order) on device-resident data: 2^30 u32 keys with u32 values and 2^29
     u64 keys with u64 values; the values are the input positions, so the result is checked by gathering the input
@@ -903,7 +948,7 @@ def main():
     ap.add_argument("--no-served", action="store_true", help="skip the serving-loop measurement")
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="--impl reference: skip timing the reference's GPU path beside its CPU sort")
-    ap.add_argument("--sweep", choices=["types", "merge", "ooc", "tune", "pairs", "generate"],
+    ap.add_argument("--sweep", choices=["types", "merge", "ooc", "tune", "pairs", "generate", "range"],
                     help="measure another workload of the sort API instead (one JSON line per case)")
     ap.add_argument("--sweep-n", type=int, default=0, help="keys per case of --sweep (0: the workload's default)")
     ap.add_argument("--tune-out", default="", help="--sweep tune: write the tuned variant table to this file")
@@ -927,6 +972,8 @@ def main():
             sweep_generate(mgs, torch, args.sweep_n or N_KEYS)
         elif args.sweep == "pairs":
             sweep_pairs(mgs, torch, args.sweep_n or (1 << 30))
+        elif args.sweep == "range":
+            sweep_range(mgs, torch, args.sweep_n or (1 << 30))
         elif args.sweep == "tune":
             sweep_tune(mgs, args.tune_out, args.sweep_n or (1 << 28))
         elif args.sweep == "merge":

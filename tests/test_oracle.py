@@ -141,3 +141,14 @@ def test_segmented_sort(orc):
     for s in range(len(offs) - 1):
         b, e = int(offs[s]), int(offs[s + 1])
         assert np.array_equal(out[b:e], np.sort(a[b:e]))
+
+
+def test_oracle_libraries_are_built_from_their_current_sources():
+    """A stale oracle library would be called with another signature: each one must be at least as new as its
+    recipe's source (rebuild with __graft_entry__.build())."""
+    import os
+    here = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle")
+    for lib, src in (("_build/liboracle.so", "oracle.cpp"), ("_ref/libref.so", "ref_wrap.cu")):
+        lp, sp = os.path.join(here, lib), os.path.join(here, src)
+        if os.path.exists(lp):
+            assert os.path.getmtime(lp) >= os.path.getmtime(sp), f"oracle/{lib} is older than oracle/{src}"
