@@ -225,7 +225,9 @@ def batched_bench(mgs, torch, ctx, dtype="u32", with_plain=True):
     out = {"segments": int(offs.size - 1), "keys": n, "dtype": dtype,
            "values": "uniform over the full range" + (", 0.1% -0.0 and 0.1% NaN" if dtype == "f32" else ""),
            "lengths": "Zipf(1.2) in [1, 2^22] rescaled to ~2^28 keys, random order",
-           "segments_le_256": int((lens <= 256).sum()), "segments_gt_16384": int((lens > 16384).sum()),
+           "segments_warp_le_1024": int((lens <= 1024).sum()),
+           "segments_cta_le_16384": int(((lens > 1024) & (lens <= 16384)).sum()),
+           "segments_onesweep_gt_16384": int((lens > 16384).sum()),
            "batched_ms": batched_ms, "batched_keys_per_s": n / (batched_ms / 1e3), "verified": verified,
            "graph_ms": graph_ms, "graph_same_result": graph_same, "kernel_ms": kernel_ms}
     if with_plain:

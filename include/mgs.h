@@ -167,8 +167,8 @@ int mgs_kway_merge_device(mgs_ctx* ctx, int dtype, const void* const* d_runs, co
  * Every segment [d_offsets[s], d_offsets[s+1]) of d_keys (device, n keys) is
  * sorted on its own, ascending and stably, in the same order as
  * mgs_sort_device. d_offsets: num_segments + 1 device uint64 values, each
- * segment inside [0, n). Segments of up to 256 keys are sorted by one warp,
- * up to one tile (16384 4-byte / 8192 8-byte keys) by one CTA entirely in
+ * segment inside [0, n). Segments of up to 1024 4-byte / 512 8-byte keys are
+ * sorted by one warp, up to one tile (16384 / 8192 keys) by one CTA entirely in
  * shared memory, both classes in one persistent launch; longer segments go
  * through the onesweep passes all at once. The launch sequence does not read
  * anything back to the host (stream-ordered, capturable in a CUDA graph).

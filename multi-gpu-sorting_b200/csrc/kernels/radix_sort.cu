@@ -604,23 +604,10 @@ struct SegLarge {
   const uint32_t* tile_prefix;        // first global tile of each large segment (n_large + 1)
   const uint32_t* counts;             // [n_small, n_medium, n_large, large_tiles]
   const uint32_t* bucket;             // [n_large][P][256] bucket starts
-  const uint32_t* tile_seg;           // large segment (index into ids) of every large tile
+  // Per large tile, its segment's {first key, keys, first tile, index into ids}, written by seg_histogram: a
+  // tile's span is one 16-byte load (first keys fit 32 bits: segmented sorts take n < 2^32).
+  const uint4* tile_info;
 };
-
-template <class Tr>
-__device__ __forceinline__ TileSpan<Tr> seg_span(const SegLarge& sg, const typename Tr::Bits* src,
-                                                 typename Tr::Bits* dst, uint32_t tile, int pass) {
-  const uint32_t lo = sg.tile_seg[tile];
-  const uint32_t seg = sg.ids[lo];
-  const unsigned long long b = sg.offsets[seg];
-  TileSpan<Tr> sp;
-  sp.src = src + b;
-  sp.dst = dst + b;
-  sp.first_tile = sg.tile_prefix[lo];
-  sp.seg_len = uint32_t(sg.offsets[seg + 1] - b);
-  sp.bucket = sg.bucket + (size_t(lo) * Tr::kPasses + pass) * kRadix;
-  return sp;
-}
 
 // The 16-byte-aligned window that covers [p, p + count): it starts at p
 // rounded down to 16 bytes and ends at p + count rounded up (the bulk copy's
@@ -680,11 +667,18 @@ __global__ __launch_bounds__(BLOCK, MINB) void radix_onesweep_kernel(typename Tr
   Bits* dst = sel ? buf0 : buf1;
   const ValueSpan<V> vspan{sel ? vbuf1 : vbuf0, sel ? vbuf0 : vbuf1};
 
-  auto span_of = [&](uint32_t t) {
-    if (SEG) return seg_span<Tr>(sg, src, dst, t, pass);
+  // A segmented tile's span comes from its 16-byte record (loaded ahead by the leader); a plain tile's span is
+  // the whole array.
+  auto span_of = [&](const uint4& rec) {
+    if (SEG) {
+      TileSpan<Tr> sp{src + rec.x, dst + rec.x, rec.z, rec.y,
+                      sg.bucket + (size_t(rec.w) * Tr::kPasses + pass) * kRadix};
+      return sp;
+    }
     TileSpan<Tr> sp{src, dst, 0u, n, st->bucket_start[pass]};
     return sp;
   };
+  auto record_of = [&](uint32_t t) { return SEG ? sg.tile_info[t] : make_uint4(0u, 0u, 0u, 0u); };
   // Tile t's keys (and values) as aligned windows of the source arrays. The
   // keys of a segment or of an unaligned buffer start anywhere; the window
   // copy still goes through the TMA, and the tile is read `shift` keys into
@@ -717,14 +711,22 @@ __global__ __launch_bounds__(BLOCK, MINB) void radix_onesweep_kernel(typename Tr
     if constexpr (kHasValues<V>) bulk_copy_g2s(sm.vals.v[b], w.v.start, w.v.bytes, &sm.bar[b]);
   };
 
-  // Persistent CTA: tiles come in launch order from an atomic counter. The
-  // next tile is claimed (and its span worked out) at the top of each
-  // iteration, and its TMA bulk copy is issued into the other buffer as soon
-  // as every warp is past the current tile's first barrier (that buffer's
-  // previous tile is then fully scattered), so loads overlap ranking. A CTA's
-  // current tile is always older than its prefetched one, so the oldest
-  // unfinished tile is always being processed and the look-back makes
-  // progress.
+  // Persistent CTA: tiles come in launch order from an atomic counter. In the
+  // plain sort the leader claims one tile ahead of the one it prefetches: at
+  // the top of each iteration the tile claimed one iteration earlier becomes
+  // the next tile and the tile after it is claimed, a result first needed one
+  // iteration later (measured on 2^30 u32 keys: 0.6 % faster per pass). The
+  // segmented sort claims the next tile at the top of the iteration and loads
+  // its span record (claiming ahead measured 8 % slower there: its tiles,
+  // partial ones among them, take unequal times, and a tile claimed ahead
+  // waits behind two of its CTA's tiles while later tiles' look-backs wait
+  // for it). After the first barrier (every warp is past it, so the other
+  // buffer's previous tile is fully scattered) the leader works out the next
+  // tile's span and issues its TMA bulk copy into the other buffer, so loads
+  // overlap ranking. A CTA's current tile is older than its prefetched one,
+  // and that one older than its claimed one, so the oldest unfinished tile is
+  // always some CTA's current tile and the look-back makes progress.
+  constexpr bool kClaimAhead = !SEG;
   static_assert(sizeof(TileSpan<Tr>) <= sizeof(sm.span[0]), "span slot");
   TileSpan<Tr>* spans = reinterpret_cast<TileSpan<Tr>*>(sm.span);
   for (int i = tid; i < kChains * 2 * kRadix; i += BLOCK) sm.masks[i] = 0u;
@@ -733,6 +735,7 @@ __global__ __launch_bounds__(BLOCK, MINB) void radix_onesweep_kernel(typename Tr
   // warp (the first eight warps run the tile scan and the look-back; a
   // segment's tile span takes a few dependent loads).
   constexpr int kLeader = BLOCK - 32;
+  uint32_t claimed = num_tiles;  // leader, kClaimAhead: the tile claimed after the prefetched one
   if (tid == kLeader) {
     mbar_init(&sm.bar[0], 1);
     mbar_init(&sm.bar[1], 1);
@@ -740,7 +743,8 @@ __global__ __launch_bounds__(BLOCK, MINB) void radix_onesweep_kernel(typename Tr
     const uint32_t t = atomicAdd(&st->tile_counter[pass], 1u);
     sm.tile_id[0] = t;
     if (t < num_tiles) {
-      const TileSpan<Tr> sp = span_of(t);
+      if (kClaimAhead) claimed = atomicAdd(&st->tile_counter[pass], 1u);
+      const TileSpan<Tr> sp = span_of(record_of(t));
       spans[0] = sp;
       const Windows w = windows_of(sp, t);
       if (w.tma) issue_copy(0, w);
@@ -754,20 +758,24 @@ __global__ __launch_bounds__(BLOCK, MINB) void radix_onesweep_kernel(typename Tr
     if (tile >= num_tiles) break;
     // Every thread read tile_id / spans of the other slot one iteration ago.
     uint32_t next_tile = num_tiles;
-    Windows next_win{};
+    uint4 next_rec = make_uint4(0u, 0u, 0u, 0u);
     if (tid == kLeader) {
-      next_tile = atomicAdd(&st->tile_counter[pass], 1u);
+      next_tile = kClaimAhead ? claimed : atomicAdd(&st->tile_counter[pass], 1u);
       sm.tile_id[cur ^ 1] = next_tile;
       if (next_tile < num_tiles) {
-        const TileSpan<Tr> sp = span_of(next_tile);
-        spans[cur ^ 1] = sp;
-        next_win = windows_of(sp, next_tile);
+        next_rec = record_of(next_tile);
+        if (kClaimAhead) claimed = atomicAdd(&st->tile_counter[pass], 1u);
       }
     }
     auto issue_next = [&] {
-      if (tid == kLeader && next_tile < num_tiles && next_win.tma) {
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        issue_copy(cur ^ 1, next_win);
+      if (tid == kLeader && next_tile < num_tiles) {
+        const TileSpan<Tr> sp = span_of(next_rec);
+        spans[cur ^ 1] = sp;
+        const Windows w = windows_of(sp, next_tile);
+        if (w.tma) {
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+          issue_copy(cur ^ 1, w);
+        }
       }
     };
     const TileSpan<Tr> span = spans[cur];
@@ -815,7 +823,8 @@ __global__ __launch_bounds__(BLOCK, MINB) void radix_onesweep_kernel(typename Tr
 // Batched segmented sort: every segment [offsets[s], offsets[s+1]) of one key
 // array is sorted on its own (stably), all segments in a fixed number of
 // launches. Segments fall into size classes:
-//   small  (2..kSmallCap keys)  one warp each, LSD passes in warp-private
+//   small  (2..one warp's share of a tile buffer: 1024 4-byte or 512 8-byte
+//          keys)                one warp each, LSD passes in warp-private
 //                               shared memory;
 //   medium (..one tile of keys) one CTA each, LSD passes entirely in shared
 //                               memory (load once, store once);
@@ -824,54 +833,119 @@ __global__ __launch_bounds__(BLOCK, MINB) void radix_onesweep_kernel(typename Tr
 //                               starts, tiles that never span segments, and a
 //                               look-back that stops at the segment's first tile.
 // Small and medium segments share one persistent launch.
-constexpr uint32_t kSmallCap = 256;  // 32 lanes x 8 keys
 
 struct SegPlanHeader {
-  uint32_t counts[4];  // n_small, n_medium, n_large, large tiles
-  uint32_t work_counter;
-  uint32_t pad[3];
+  uint32_t counts[4];     // n_small, n_medium, n_large, large tiles
+  uint32_t work_counter;  // next medium segment (one CTA each)
+  uint32_t small_counter; // next small segment (one warp each)
+  uint32_t pad[2];
 };
 
-template <int BLOCK>
+// Classifies the segments (ids in segment order per class) and lays out the
+// large segments' tiles. One CTA; thread t of a round classifies ITEMS
+// consecutive segments, and one block scan per round (of the three class
+// counts packed into one 64-bit word, 21 bits each, and the tile count) places
+// them, so a round covers BLOCK x ITEMS segments.
+template <int BLOCK, int ITEMS>
 __global__ __launch_bounds__(BLOCK) void seg_classify_kernel(const unsigned long long* __restrict__ offsets,
                                                              uint32_t nseg, unsigned long long n, uint32_t tile,
-                                                             uint32_t medium_cap, SegPlanHeader* __restrict__ hdr,
+                                                             uint32_t small_cap, uint32_t medium_cap,
+                                                             SegPlanHeader* __restrict__ hdr,
                                                              uint32_t* __restrict__ small_ids,
                                                              uint32_t* __restrict__ medium_ids,
                                                              uint32_t* __restrict__ large_ids,
                                                              uint32_t* __restrict__ tile_prefix,
                                                              uint32_t* __restrict__ d_status) {
-  __shared__ uint32_t tmp[BLOCK / 32 + 1];
+  constexpr int kWarps = BLOCK / 32;
+  constexpr int kField = 21;
+  static_assert(BLOCK * ITEMS < (1 << kField), "a round's class counts must fit their fields");
+  constexpr unsigned long long kFieldMask = (1ull << kField) - 1;
+  __shared__ unsigned long long s_cls[kWarps];
+  __shared__ uint32_t s_tiles[kWarps];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   uint32_t cnt_small = 0, cnt_medium = 0, cnt_large = 0, tiles = 0;
-  for (uint32_t base = 0; base < nseg; base += BLOCK) {
-    const uint32_t s = base + threadIdx.x;
-    unsigned long long len = 0;
-    if (s < nseg) {
-      const unsigned long long b = offsets[s], e = offsets[s + 1];
-      if (e < b || e > n) {
-        if (d_status) atomicOr(d_status, kStatusBadInput);
-      } else {
-        len = e - b;
+  for (uint64_t base = 0; base < nseg; base += uint64_t(BLOCK) * ITEMS) {
+    const uint64_t s0 = base + uint64_t(threadIdx.x) * ITEMS;
+    int cls[ITEMS];
+    uint32_t seg_tiles[ITEMS];
+    unsigned long long packed = 0;
+    uint32_t my_tiles = 0;
+    unsigned long long b = s0 < nseg ? offsets[s0] : 0ull;
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+      unsigned long long len = 0;
+      if (s0 + j < nseg) {
+        const unsigned long long e = offsets[s0 + j + 1];
+        if (e < b || e > n) {
+          if (d_status) atomicOr(d_status, kStatusBadInput);
+        } else {
+          len = e - b;
+        }
+        b = e;
+      }
+      cls[j] = len <= 1 ? 0 : len <= small_cap ? 1 : len <= medium_cap ? 2 : 3;
+      seg_tiles[j] = cls[j] == 3 ? uint32_t((len + tile - 1) / tile) : 0u;
+      packed += cls[j] == 0 ? 0ull : 1ull << (kField * (cls[j] - 1));
+      my_tiles += seg_tiles[j];
+    }
+    unsigned long long pin = packed;
+    uint32_t tin = my_tiles;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const unsigned long long pu = __shfl_up_sync(0xFFFFFFFFu, pin, off);
+      const uint32_t tu = __shfl_up_sync(0xFFFFFFFFu, tin, off);
+      if (lane >= off) {
+        pin += pu;
+        tin += tu;
       }
     }
-    const int cls = len <= 1 ? 0 : len <= kSmallCap ? 1 : len <= medium_cap ? 2 : 3;
-    uint32_t tot;
-    uint32_t ex = block_exclusive_scan<BLOCK>(cls == 1 ? 1u : 0u, tmp, &tot);
-    if (cls == 1) small_ids[cnt_small + ex] = s;
-    cnt_small += tot;
-    ex = block_exclusive_scan<BLOCK>(cls == 2 ? 1u : 0u, tmp, &tot);
-    if (cls == 2) medium_ids[cnt_medium + ex] = s;
-    cnt_medium += tot;
-    const uint32_t my_tiles = cls == 3 ? uint32_t((len + tile - 1) / tile) : 0u;
-    uint32_t ttot;
-    const uint32_t tex = block_exclusive_scan<BLOCK>(my_tiles, tmp, &ttot);
-    ex = block_exclusive_scan<BLOCK>(cls == 3 ? 1u : 0u, tmp, &tot);
-    if (cls == 3) {
-      large_ids[cnt_large + ex] = s;
-      tile_prefix[cnt_large + ex] = tiles + tex;
+    if (lane == 31) {
+      s_cls[warp] = pin;
+      s_tiles[warp] = tin;
     }
-    cnt_large += tot;
+    __syncthreads();
+    if (warp == 0) {
+      unsigned long long wp = lane < kWarps ? s_cls[lane] : 0ull;
+      uint32_t wt = lane < kWarps ? s_tiles[lane] : 0u;
+#pragma unroll
+      for (int off = 1; off < 32; off <<= 1) {
+        const unsigned long long pu = __shfl_up_sync(0xFFFFFFFFu, wp, off);
+        const uint32_t tu = __shfl_up_sync(0xFFFFFFFFu, wt, off);
+        if (lane >= off) {
+          wp += pu;
+          wt += tu;
+        }
+      }
+      if (lane < kWarps) {
+        s_cls[lane] = wp;
+        s_tiles[lane] = wt;
+      }
+    }
+    __syncthreads();
+    const unsigned long long pex = (warp ? s_cls[warp - 1] : 0ull) + pin - packed;
+    uint32_t xt = tiles + (warp ? s_tiles[warp - 1] : 0u) + tin - my_tiles;
+    const unsigned long long ptot = s_cls[kWarps - 1];
+    const uint32_t ttot = s_tiles[kWarps - 1];
+    uint32_t xs = cnt_small + uint32_t(pex & kFieldMask);
+    uint32_t xm = cnt_medium + uint32_t((pex >> kField) & kFieldMask);
+    uint32_t xl = cnt_large + uint32_t(pex >> (2 * kField));
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+      const uint32_t s = uint32_t(s0 + j);
+      if (cls[j] == 1) small_ids[xs++] = s;
+      if (cls[j] == 2) medium_ids[xm++] = s;
+      if (cls[j] == 3) {
+        large_ids[xl] = s;
+        tile_prefix[xl] = xt;
+        ++xl;
+        xt += seg_tiles[j];
+      }
+    }
+    cnt_small += uint32_t(ptot & kFieldMask);
+    cnt_medium += uint32_t((ptot >> kField) & kFieldMask);
+    cnt_large += uint32_t(ptot >> (2 * kField));
     tiles += ttot;
+    __syncthreads();  // s_cls / s_tiles are rewritten by the next round
   }
   if (threadIdx.x == 0) {
     tile_prefix[cnt_large] = tiles;
@@ -880,33 +954,32 @@ __global__ __launch_bounds__(BLOCK) void seg_classify_kernel(const unsigned long
     hdr->counts[2] = cnt_large;
     hdr->counts[3] = tiles;
     hdr->work_counter = 0;
+    hdr->small_counter = 0;
   }
 }
 
-// Sorts one small segment (len <= kSmallCap) with one warp: LSD passes of
-// 8-bit digits between two warp-private shared buffers; passes whose digit is
-// the same for every key are skipped.
-template <class Tr>
+// Sorts one small segment (len <= CAP) with one warp: LSD passes of 8-bit
+// digits between two warp-private shared buffers of CAP keys; passes whose
+// digit is the same for every key are skipped. Each pass counts the digits
+// (shared atomics), scans the 256 counters across the lanes, then places the
+// keys 32 at a time in index order: the lanes holding one digit find each
+// other through a shared bit mask, take consecutive slots in lane order, and
+// the highest of them advances the digit's counter (stable).
+template <class Tr, uint32_t CAP>
 __device__ __forceinline__ void warp_sort_small(typename Tr::Bits* __restrict__ keys, uint32_t len,
                                                 typename Tr::Bits* A, typename Tr::Bits* B, uint32_t* cnt,
                                                 uint32_t* mm) {
   using Bits = typename Tr::Bits;
-  constexpr int kItems = kSmallCap / 32;
   const int lane = threadIdx.x & 31;
   const uint32_t lmask = lanemask_lt(), lmask_gt = lanemask_gt();
+  const uint32_t steps = (len + 31) / 32;
   for (uint32_t i = lane; i < len; i += 32) A[i] = keys[i];
   __syncwarp();
   for (int pass = 0; pass < Tr::kPasses; ++pass) {
 #pragma unroll
     for (int q = 0; q < 8; ++q) cnt[lane * 8 + q] = 0u;
     __syncwarp();
-    Bits k[kItems];
-#pragma unroll
-    for (int j = 0; j < kItems; ++j) {
-      const uint32_t idx = j * 32 + lane;
-      k[j] = A[idx];
-      if (idx < len) atomicAdd(&cnt[Tr::Digit(k[j], pass)], 1u);
-    }
+    for (uint32_t i = lane; i < len; i += 32) atomicAdd(&cnt[Tr::Digit(A[i], pass)], 1u);
     __syncwarp();
     uint32_t c[8], local = 0;
     bool uniform = false;
@@ -933,11 +1006,11 @@ __device__ __forceinline__ void warp_sort_small(typename Tr::Bits* __restrict__ 
       continue;  // identity permutation
     }
     __syncwarp();
-#pragma unroll
-    for (int j = 0; j < kItems; ++j) {
+    for (uint32_t j = 0; j < steps; ++j) {
       const uint32_t idx = j * 32 + lane;
       const bool ok = idx < len;
-      const uint32_t d = ok ? Tr::Digit(k[j], pass) : 0u;
+      const Bits k = ok ? A[idx] : Bits(0);
+      const uint32_t d = ok ? Tr::Digit(k, pass) : 0u;
       uint32_t* m = mm + (j & 1) * kRadix;
       if (ok) atomicOr(&m[d], 1u << lane);
       __syncwarp();
@@ -949,7 +1022,7 @@ __device__ __forceinline__ void warp_sort_small(typename Tr::Bits* __restrict__ 
         m[d] = 0u;
       }
       __syncwarp();
-      if (ok && pos < kSmallCap) B[pos] = k[j];
+      if (ok && pos < CAP) B[pos] = k;
     }
     __syncwarp();
     Bits* t = A;
@@ -960,6 +1033,18 @@ __device__ __forceinline__ void warp_sort_small(typename Tr::Bits* __restrict__ 
   __syncwarp();
 }
 
+// Keys a warp sorts alone in the segmented sort: one warp's share of a tile
+// buffer (1024 4-byte or 512 8-byte keys with the default 512 x 32 / 512 x 16
+// tiles).
+template <class Tr>
+constexpr uint32_t seg_small_cap() {
+  using Shape = OnesweepShape<sizeof(typename Tr::Bits), kDefaultShape>;
+  return uint32_t(Shape::kItems) * 32u;
+}
+
+// Medium segments first, one CTA each (grabbed through work_counter), then
+// small segments, one warp each (grabbed per warp through small_counter, so a
+// warp never waits for the others of its CTA).
 template <class Tr, int BLOCK, int ITEMS, int MINB, int CHAINS, int MATCH>
 __global__ __launch_bounds__(BLOCK, MINB) void seg_small_medium_kernel(typename Tr::Bits* __restrict__ keys,
                                                                        const unsigned long long* __restrict__ offsets,
@@ -970,95 +1055,169 @@ __global__ __launch_bounds__(BLOCK, MINB) void seg_small_medium_kernel(typename 
   using Smem = OnesweepSmem<Tr, BLOCK, ITEMS, CHAINS>;
   constexpr int kWarps = BLOCK / 32;
   constexpr int kChains = Smem::kChains;
-  static_assert(kWarps * kSmallCap <= Smem::kTile, "warp buffers fit in one tile buffer");
+  constexpr uint32_t kCap = uint32_t(ITEMS) * 32u;
+  static_assert(kWarps * kCap <= Smem::kTile, "warp buffers fit in one tile buffer");
   static_assert(CHAINS == 1, "one mask/counter region per warp");
   extern __shared__ __align__(128) unsigned char smem_raw[];
   Smem& sm = *reinterpret_cast<Smem*>(smem_raw);
   __shared__ uint32_t s_work;
-  const int tid = threadIdx.x, warp = tid >> 5;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   for (int i = tid; i < kChains * 2 * kRadix; i += BLOCK) sm.masks[i] = 0u;
   const uint32_t n_small = hdr->counts[0], n_medium = hdr->counts[1];
-  const uint32_t n_items = n_medium + (n_small + kWarps - 1) / kWarps;
   for (;;) {
     __syncthreads();
     if (tid == 0) s_work = atomicAdd(&hdr->work_counter, 1u);
     __syncthreads();
     const uint32_t work = s_work;
-    if (work >= n_items) break;
-    if (work < n_medium) {
-      const uint32_t seg = medium_ids[work];
-      const unsigned long long b = offsets[seg];
-      const uint32_t len = uint32_t(offsets[seg + 1] - b);
-      Bits* g = keys + b;
-      for (uint32_t i = tid; i < len; i += BLOCK) sm.keys[0][i] = g[i];
-      const uint32_t span = (len + BLOCK - 1) / BLOCK;  // keys per lane: every warp takes a share
-      int cur = 0;
-      for (int pass = 0; pass < Tr::kPasses; ++pass) {
-        uint32_t tc;
-        const bool skipped = rank_tile<Tr, BLOCK, ITEMS, CHAINS, MATCH, false, true, true>(
-            sm, sm.keys[cur], sm.keys[cur ^ 1], len, pass, &tc, [](uint32_t) {}, [](uint32_t) {},
-            static_cast<const NoValue*>(nullptr), static_cast<NoValue*>(nullptr), PlainDigits{}, span);
-        __syncthreads();
-        if (!skipped) cur ^= 1;
-      }
-      for (uint32_t i = tid; i < len; i += BLOCK) g[i] = sm.keys[cur][i];
-    } else {
-      const uint32_t idx = (work - n_medium) * kWarps + warp;
-      if (idx < n_small) {
-        const uint32_t seg = small_ids[idx];
-        const unsigned long long b = offsets[seg];
-        warp_sort_small<Tr>(keys + b, uint32_t(offsets[seg + 1] - b), sm.keys[0] + warp * kSmallCap,
-                            sm.keys[1] + warp * kSmallCap, sm.ccount + warp * kRadix, sm.masks + warp * 2 * kRadix);
-      }
+    if (work >= n_medium) break;
+    const uint32_t seg = medium_ids[work];
+    const unsigned long long b = offsets[seg];
+    const uint32_t len = uint32_t(offsets[seg + 1] - b);
+    Bits* g = keys + b;
+    for (uint32_t i = tid; i < len; i += BLOCK) sm.keys[0][i] = g[i];
+    const uint32_t span = (len + BLOCK - 1) / BLOCK;  // keys per lane: every warp takes a share
+    int cur = 0;
+    for (int pass = 0; pass < Tr::kPasses; ++pass) {
+      uint32_t tc;
+      const bool skipped = rank_tile<Tr, BLOCK, ITEMS, CHAINS, MATCH, false, true, true>(
+          sm, sm.keys[cur], sm.keys[cur ^ 1], len, pass, &tc, [](uint32_t) {}, [](uint32_t) {},
+          static_cast<const NoValue*>(nullptr), static_cast<NoValue*>(nullptr), PlainDigits{}, span);
+      __syncthreads();
+      if (!skipped) cur ^= 1;
     }
+    for (uint32_t i = tid; i < len; i += BLOCK) g[i] = sm.keys[cur][i];
+  }
+  for (;;) {
+    uint32_t idx = 0;
+    if (lane == 0) idx = atomicAdd(&hdr->small_counter, 1u);
+    idx = __shfl_sync(0xFFFFFFFFu, idx, 0);
+    if (idx >= n_small) break;
+    const uint32_t seg = small_ids[idx];
+    const unsigned long long b = offsets[seg];
+    warp_sort_small<Tr, kCap>(keys + b, uint32_t(offsets[seg + 1] - b), sm.keys[0] + warp * kCap,
+                              sm.keys[1] + warp * kCap, sm.ccount + warp * kRadix, sm.masks + warp * 2 * kRadix);
   }
 }
 
 // Per large segment and pass: digit counts (one read of the large segments),
-// the segment of every large tile (for the onesweep's tile spans), and the
-// first look-back array cleared.
-template <class Tr, int BLOCK>
-__global__ __launch_bounds__(BLOCK) void seg_histogram_kernel(const typename Tr::Bits* __restrict__ keys,
-                                                              SegLarge sg, uint32_t tile,
-                                                              uint32_t* __restrict__ seg_hist,
-                                                              uint32_t* __restrict__ lb0,
-                                                              uint32_t* __restrict__ tile_seg) {
+// the span of every large tile (tile_info, for the onesweep kernels), and the
+// first look-back array cleared. One CTA per SM; CTA b of G takes the
+// contiguous large tiles [b T / G, (b + 1) T / G) (T large tiles in all), so
+// its range crosses only a few segment boundaries. Keys are counted into
+// per-lane histogram copies (the layout of radix_histogram: no bank conflicts
+// whatever the digits) with 16-byte streaming loads, and the copies are folded
+// into the segment's global histogram, and cleared, each time the range
+// leaves a segment. The next segment's bounds are fetched while the current
+// one is counted.
+template <class Tr, class Dg>
+__global__ __launch_bounds__(kHistBlock, 1) void seg_histogram_kernel(const typename Tr::Bits* __restrict__ keys,
+                                                                   SegLarge sg, uint32_t tile,
+                                                                   uint32_t* __restrict__ seg_hist,
+                                                                   uint32_t* __restrict__ lb0,
+                                                                   uint4* __restrict__ tile_info, Dg dg) {
   using Bits = typename Tr::Bits;
   constexpr int P = Tr::kPasses;
-  __shared__ uint32_t h[P * kRadix];
-  __shared__ uint32_t s_seg, s_first;
+  constexpr int C = HistCopies<Tr>::kCopies;
+  constexpr int kCounters = P * kRadix;
+  constexpr int kVecsPerCounter = C / 4;  // 16-byte words holding one counter's copies
+  constexpr int kRotDiv = 32 / C;         // see the fold below
+  constexpr int kPerVec = 16 / int(sizeof(Bits));
+  extern __shared__ __align__(16) uint32_t hist_smem[];
+  uint4* const rows = reinterpret_cast<uint4*>(hist_smem);
+
   const uint32_t num_tiles = sg.counts[3];
-  for (size_t i = size_t(blockIdx.x) * BLOCK + threadIdx.x; i < size_t(num_tiles) * kRadix;
-       i += size_t(gridDim.x) * BLOCK)
+  const uint32_t n_large = sg.counts[2];
+  for (size_t i = size_t(blockIdx.x) * kHistBlock + threadIdx.x; i < size_t(num_tiles) * kRadix;
+       i += size_t(gridDim.x) * kHistBlock)
     lb0[i] = 0u;
-  for (uint32_t t = blockIdx.x; t < num_tiles; t += gridDim.x) {
-    for (int i = threadIdx.x; i < P * kRadix; i += BLOCK) h[i] = 0u;
-    if (threadIdx.x == 0) {
-      uint32_t lo = 0, hi = sg.counts[2];
-      while (hi - lo > 1) {
-        const uint32_t mid = (lo + hi) >> 1;
-        if (sg.tile_prefix[mid] <= t) lo = mid; else hi = mid;
-      }
-      s_seg = lo;
-      s_first = sg.tile_prefix[lo];
-      tile_seg[t] = lo;
-    }
-    __syncthreads();
-    const uint32_t si = s_seg;
-    const unsigned long long b = sg.offsets[sg.ids[si]];
-    const uint32_t len = uint32_t(sg.offsets[sg.ids[si] + 1] - b);
-    const uint32_t off = (t - s_first) * tile;
-    const uint32_t cnt = min(tile, len - off);
-    const Bits* src = keys + b + off;
-    for (uint32_t i = threadIdx.x; i < cnt; i += BLOCK) {
-      const Bits o = Tr::Ordered(src[i]);
+  const uint32_t t0 = uint32_t(uint64_t(num_tiles) * blockIdx.x / gridDim.x);
+  const uint32_t t1 = uint32_t(uint64_t(num_tiles) * (blockIdx.x + 1) / gridDim.x);
+  if (t0 >= t1) return;  // the whole CTA
+  for (int i = threadIdx.x; i < kCounters * kVecsPerCounter; i += kHistBlock) rows[i] = make_uint4(0u, 0u, 0u, 0u);
+
+  // The large segment holding tile t0: the largest s with tile_prefix[s] <= t0
+  // (tile_prefix is strictly increasing, every large segment has two tiles or
+  // more). Each round probes kHistBlock evenly spaced entries at once.
+  uint32_t lo = 0, hi = n_large;
+  while (hi - lo > 1) {
+    const uint32_t step = (hi - lo + kHistBlock - 1) / kHistBlock;
+    const uint32_t j = lo + (threadIdx.x + 1) * step;
+    const uint32_t c = uint32_t(__syncthreads_count(j < hi && sg.tile_prefix[j] <= t0));
+    lo += c * step;
+    hi = min(hi, lo + step);
+  }
+
+  struct Seg {
+    uint32_t begin, len, first, end;  // first key; keys; first tile; one past the last tile
+  };
+  auto seg_at = [&](uint32_t s) {
+    const uint32_t id = sg.ids[s];
+    const unsigned long long b = sg.offsets[id];
+    return Seg{uint32_t(b), uint32_t(sg.offsets[id + 1] - b), sg.tile_prefix[s], sg.tile_prefix[s + 1]};
+  };
+  uint32_t* const copy = hist_smem + (threadIdx.x & (C - 1));
+  auto count_key = [&](Bits k) {
 #pragma unroll
-      for (int p = 0; p < P; ++p) atomicAdd(&h[p * kRadix + (uint32_t(o >> (8 * p)) & 0xFFu)], 1u);
+    for (int p = 0; p < P; ++p) atomicAdd(copy + (p * kRadix + dg.template digit<Tr>(k, p)) * C, 1u);
+  };
+
+  uint32_t si = lo;
+  Seg cur = seg_at(si);
+  __syncthreads();  // copies cleared
+  for (uint32_t t = t0; t < t1;) {
+    const uint32_t ct1 = min(t1, cur.end);
+    const Seg nxt = ct1 < t1 ? seg_at(si + 1) : cur;
+    for (uint32_t x = t + threadIdx.x; x < ct1; x += kHistBlock)
+      tile_info[x] = make_uint4(cur.begin, cur.len, cur.first, si);
+    const uint32_t k0 = (t - cur.first) * tile;
+    const uint32_t cnt = min(cur.len, (ct1 - cur.first) * tile) - k0;
+    const Bits* const src = keys + cur.begin + k0;
+    const uint32_t head =
+        min(cnt, uint32_t(((16u - (reinterpret_cast<uintptr_t>(src) & 15u)) & 15u) / sizeof(Bits)));
+    const uint32_t nvec = (cnt - head) / kPerVec;
+    const uint32_t tail = head + nvec * kPerVec;
+    if (threadIdx.x < head) count_key(src[threadIdx.x]);
+    if (threadIdx.x < cnt - tail) count_key(src[tail + threadIdx.x]);
+    const uint4* kv = reinterpret_cast<const uint4*>(src + head);
+    uint32_t v = threadIdx.x;
+    for (; v + (kHistUnroll - 1) * kHistBlock < nvec; v += kHistUnroll * kHistBlock) {
+      uint4 q[kHistUnroll];
+#pragma unroll
+      for (int u = 0; u < kHistUnroll; ++u) q[u] = ld_stream_v4(kv + v + u * kHistBlock);
+#pragma unroll
+      for (int u = 0; u < kHistUnroll; ++u) {
+        Bits k[kPerVec];
+        unpack_v4<Bits>(q[u], k);
+#pragma unroll
+        for (int j = 0; j < kPerVec; ++j) count_key(k[j]);
+      }
+    }
+    for (; v < nvec; v += kHistBlock) {
+      Bits k[kPerVec];
+      unpack_v4<Bits>(ld_stream_v4(kv + v), k);
+#pragma unroll
+      for (int j = 0; j < kPerVec; ++j) count_key(k[j]);
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < P * kRadix; i += BLOCK)
-      if (h[i]) atomicAdd(&seg_hist[size_t(si) * P * kRadix + i], h[i]);
+    // Fold: thread r sums counter r's C copies (kVecsPerCounter 16-byte words)
+    // and clears them. The words are visited in a rotated order so that the 8
+    // threads of each quarter-warp touch 8 different 16-byte bank groups.
+    for (int r = threadIdx.x; r < kCounters; r += kHistBlock) {
+      uint4* const row = rows + r * kVecsPerCounter;
+      uint32_t sum = 0u;
+#pragma unroll
+      for (int q = 0; q < kVecsPerCounter; ++q) {
+        const int w = (q + r / kRotDiv) & (kVecsPerCounter - 1);
+        const uint4 c4 = row[w];
+        row[w] = make_uint4(0u, 0u, 0u, 0u);
+        sum += c4.x + c4.y + c4.z + c4.w;
+      }
+      if (sum) atomicAdd(&seg_hist[size_t(si) * kCounters + r], sum);
+    }
     __syncthreads();
+    t = ct1;
+    ++si;
+    cur = nxt;
   }
 }
 
@@ -1413,7 +1572,7 @@ cudaError_t radix_sort_typed(typename Tr::Bits* keys, size_t n, void* temp, size
 // ---------------------------------------------------------------- segmented host
 struct SegLayout {
   size_t state_off, hdr_off, small_off, medium_off, large_off, prefix_off, hist_off, bucket_off, lb0_off, lb1_off,
-      tile_seg_off, keys_off, total;
+      tile_info_off, keys_off, total;
   size_t max_large, max_tiles, hist_bytes;
 };
 
@@ -1441,7 +1600,7 @@ SegLayout seg_layout(size_t n, size_t nseg) {
   L.bucket_off = take(L.hist_bytes);
   L.lb0_off = take(L.max_tiles * kRadix * 4);
   L.lb1_off = take(L.max_tiles * kRadix * 4);
-  L.tile_seg_off = take(L.max_tiles * 4);
+  L.tile_info_off = take(L.max_tiles * 16);
   L.keys_off = take(n * sizeof(typename Tr::Bits));
   L.total = off;
   return L;
@@ -1469,16 +1628,16 @@ cudaError_t segmented_sort_typed(typename Tr::Bits* keys, size_t n, const uint64
   uint32_t* hist = reinterpret_cast<uint32_t*>(tb + L.hist_off);
   uint32_t* bucket = reinterpret_cast<uint32_t*>(tb + L.bucket_off);
   uint32_t* lb[2] = {reinterpret_cast<uint32_t*>(tb + L.lb0_off), reinterpret_cast<uint32_t*>(tb + L.lb1_off)};
-  uint32_t* tile_seg = reinterpret_cast<uint32_t*>(tb + L.tile_seg_off);
+  uint4* tile_info = reinterpret_cast<uint4*>(tb + L.tile_info_off);
   Bits* tmp = reinterpret_cast<Bits*>(tb + L.keys_off);
   const unsigned long long* offs = reinterpret_cast<const unsigned long long*>(d_offsets);
 
   cudaError_t e = cudaMemsetAsync(tb, 0, L.small_off, stream);  // RadixState + plan header
   if (e == cudaSuccess && L.hist_bytes) e = cudaMemsetAsync(hist, 0, L.hist_bytes, stream);
   if (e != cudaSuccess) return e;
-  e = launch_kernel(rec, "seg_classify", seg_classify_kernel<1024>, dim3(1), dim3(1024), 0, stream, offs,
-                    uint32_t(nseg), (unsigned long long)n, kTile, kTile, hdr, small_ids, medium_ids, large_ids,
-                    prefix, d_status);
+  e = launch_kernel(rec, "seg_classify", seg_classify_kernel<1024, 8>, dim3(1), dim3(1024), 0, stream, offs,
+                    uint32_t(nseg), (unsigned long long)n, kTile, seg_small_cap<Tr>(), kTile, hdr, small_ids,
+                    medium_ids, large_ids, prefix, d_status);
   if (e != cudaSuccess) return e;
 
   const int sms = device_sm_count();
@@ -1492,10 +1651,16 @@ cudaError_t segmented_sort_typed(typename Tr::Bits* keys, size_t n, const uint64
                       static_cast<const uint32_t*>(medium_ids));
     if (e != cudaSuccess) return e;
   }
-  SegLarge sg{offs, large_ids, prefix, hdr->counts, bucket, tile_seg};
-  e = launch_kernel(rec, "seg_histogram", seg_histogram_kernel<Tr, 256>, dim3(unsigned(sms * 4)), dim3(256), 0,
-                    stream, static_cast<const Bits*>(keys), sg, kTile, hist, lb[0], tile_seg);
-  if (e != cudaSuccess) return e;
+  SegLarge sg{offs, large_ids, prefix, hdr->counts, bucket, tile_info};
+  {
+    auto kernel = seg_histogram_kernel<Tr, PlainDigits>;
+    static SmemLimitOnce attr;
+    e = attr.ensure(kernel, HistCopies<Tr>::kSmemBytes);
+    if (e != cudaSuccess) return e;
+    e = launch_kernel(rec, "seg_histogram", kernel, dim3(unsigned(sms)), dim3(kHistBlock), HistCopies<Tr>::kSmemBytes,
+                      stream, static_cast<const Bits*>(keys), sg, kTile, hist, lb[0], tile_info, PlainDigits{});
+    if (e != cudaSuccess) return e;
+  }
   e = launch_kernel(rec, "seg_scan", seg_scan_kernel<Tr::kPasses>, dim3(unsigned(sms * 4)), dim3(kRadix), 0, stream,
                     static_cast<const uint32_t*>(hdr->counts), static_cast<const uint32_t*>(hist), bucket);
   if (e != cudaSuccess) return e;

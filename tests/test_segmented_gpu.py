@@ -81,6 +81,26 @@ def test_zipf_segment_lengths(ctx, mgs, orc, dtype):
     assert got.tobytes() == orc.segmented_sort(a, offs).tobytes()
 
 
+@pytest.mark.parametrize("dtype", ["u32", "i64"])
+def test_classify_rounds_and_histogram_ranges(ctx, mgs, orc, dtype):
+    """Over 3 x 8192 segments, so the classification takes several rounds, with large segments placed at the
+    round edges; more large tiles than SMs, so the histogram's per-CTA tile ranges start inside segments and
+    cross several of them; segment starts at every alignment."""
+    rng = np.random.default_rng(13)
+    w = mgs.np_dtype(dtype).itemsize
+    tile = 16384 if w == 4 else 8192
+    nseg = 3 * 8192 + 5
+    lengths = rng.integers(0, 300, nseg)
+    for i, s in enumerate([0, 8191, 8192, 8193, 16383, 16384, 24575, 24576, nseg - 1]):
+        lengths[s] = [tile + 1, 3 * tile + 7, 2 * tile, 40 * tile + 3, tile + 5, 7 * tile, 2 * tile + 1,
+                      100 * tile - 1, 5 * tile + 2][i]
+    offs = layout(rng, lengths)
+    n = int(offs[-1])
+    a = mgs.generate(dtype, "full-uniform", 17, n)
+    got = run_segmented(ctx, mgs, a, offs, dtype)
+    assert got.tobytes() == orc.segmented_sort(a, offs).tobytes()
+
+
 def test_single_segment_equals_device_sort(ctx, mgs, orc):
     a = mgs.generate("u32", "uniform", 3, 1_000_003)
     got = run_segmented(ctx, mgs, a, [0, a.size], "u32")
