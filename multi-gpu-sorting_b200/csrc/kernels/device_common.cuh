@@ -81,6 +81,18 @@ struct RangeDigits {
   }
 };
 
+// Digits of the ordered key minus `base`, for 4-byte keys whose ordered values
+// all lie in [base, base + 2^(8 * passes)): a k-way merge tile whose keys span
+// a narrow range is sorted by that many passes.
+struct OffsetDigits {
+  uint32_t base;
+  template <class Tr>
+  __device__ __forceinline__ uint32_t digit(typename Tr::Bits k, int pass) const {
+    static_assert(sizeof(typename Tr::Bits) == 4, "4-byte keys");
+    return ((uint32_t(Tr::Ordered(k)) - base) >> (8 * pass)) & 0xFFu;
+  }
+};
+
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }

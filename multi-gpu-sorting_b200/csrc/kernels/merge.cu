@@ -10,7 +10,8 @@
 //                        warp per output tile boundary: bisection over the radix
 //                        order key space, every lane narrowing the index window of
 //                        its runs, then ties split by run index (stable).
-//                        Hierarchical: a coarse level bounds the fine searches.
+//                        Hierarchical: coarser levels (every 256, then every
+//                        16 tiles) bound the finer searches.
 //   K5/K7b tile_merge  : per output tile, the k input ranges are staged in shared
 //                        memory in run order and merged by ceil(log2 k) rounds of
 //                        pairwise merge-path merges in shared memory, then stored
@@ -20,12 +21,14 @@
 // Order: radix order of the keys (KeyTraits::Ordered); on ties the lower run
 // (the first range) comes first.
 #include <algorithm>
+#include <cstdlib>
 #include <mutex>
 #include <vector>
 
 #include "device_common.cuh"
 #include "dispatch.cuh"
 #include "merge.cuh"
+#include "radix_sort.cuh"
 
 namespace mgs {
 namespace {
@@ -111,6 +114,7 @@ __device__ __forceinline__ u64 bound_search(const typename Tr::Bits* run, u64 lo
 }
 
 constexpr int kMaxRunsPerLane = kMaxKwayRuns / 32;
+static_assert(kMaxKwayTileRuns >= kMaxKwayRuns, "the radix tiles take every k-way merge");
 
 // One warp per diagonal d: splits[r] = number of elements of run r among the
 // first d outputs of the stable k-way merge. Optional coarse level: the
@@ -459,21 +463,59 @@ int merge_shape(int k) {
   return k <= 2 ? 0 : 1;
 }
 
-constexpr u64 kCoarseTiles = 256;  // fine tiles per coarse diagonal
+// The C ABI dtype of a key traits type.
+template <class Tr>
+constexpr int dtype_of() {
+  return (sizeof(typename Tr::Bits) == 4 ? 0 : 3) + Tr::kKind;
+}
+
+// Merges of at least this many runs of 4-byte keys sort their output tiles in
+// shared memory (kway_radix_tiles: 16384-key tiles, range-limited LSD passes,
+// two for uniform keys) instead of ceil(log2 k) pairwise merge rounds over
+// 8192-key tiles. Measured on a B200, 2^31 u32 keys in Dirichlet(1) runs,
+// sorted tiles against merged tiles (partition included): k = 8: 18.2 / 14.8
+// ms, 16: 18.9 / 18.3, 32: 21.4 / 24.6, 64: 25.2 / 32.8. MGS_KWAY_RADIX_MIN_RUNS
+// overrides it for experiments (0: never).
+int kway_radix_min_runs() {
+  static const int env = [] {
+    const char* e = getenv("MGS_KWAY_RADIX_MIN_RUNS");
+    return e ? atoi(e) : -1;
+  }();
+  return env >= 0 ? (env == 0 ? kMaxKwayRuns + 1 : env) : 24;
+}
+
+// Output tile of a k-way merge: a radix tile or a merge tile.
+template <class Tr>
+u64 kway_tile_keys(int k, bool* radix) {
+  const size_t rt = kway_radix_tile_keys(dtype_of<Tr>());
+  *radix = k > 2 && rt != 0 && k >= kway_radix_min_runs();
+  return *radix ? u64(rt) : merge_tile_keys(sizeof(typename Tr::Bits), merge_shape(k));
+}
+
+// The exact splits of a k-way merge (k > 2) are found level by level: every
+// 256 output tiles, then every 16 tiles within those bounds, then at every
+// tile boundary within those. A level bounds the next one's value bisection
+// and per-run index windows, so the fine searches start from windows of about
+// 16 tiles / k keys per run. A level exists only when the merge spans more
+// than two of its spacings. Measured on a B200, 2^31 u32 keys, k = 64: the
+// partition took 6.3 ms with the 256-tile level alone.
+constexpr int kBoundLevels = 2;
+constexpr u64 kBoundTiles[kBoundLevels] = {256, 16};  // tiles per diagonal of each bounding level
 
 struct KwayLayout {
-  size_t ptrs_off, lens_off, splits_off, c_splits_off, c_ub_off, c_lt_off, c_vstar_off, total;
-  u64 num_tiles, num_coarse;
-  bool coarse;
+  size_t ptrs_off, lens_off, splits_off, total;
+  size_t b_splits_off[kBoundLevels], b_ub_off[kBoundLevels], b_lt_off[kBoundLevels], b_vstar_off[kBoundLevels];
+  u64 tile, num_tiles;
+  u64 b_diag[kBoundLevels];  // diagonals of each bounding level (0: level absent)
+  bool radix;
 };
 
 template <class Tr>
 KwayLayout kway_layout(int k, size_t total) {
-  const u64 kTile = merge_tile_keys(sizeof(typename Tr::Bits), merge_shape(k));
   KwayLayout L;
+  const u64 kTile = kway_tile_keys<Tr>(k, &L.radix);
+  L.tile = kTile;
   L.num_tiles = (total + kTile - 1) / kTile;
-  L.coarse = (k > 2) && (L.num_tiles > 2 * kCoarseTiles);
-  L.num_coarse = L.coarse ? (total + kTile * kCoarseTiles - 1) / (kTile * kCoarseTiles) : 0;
   size_t off = 0;
   L.ptrs_off = off;
   off += align_up(size_t(k) * 8, 256);
@@ -481,15 +523,20 @@ KwayLayout kway_layout(int k, size_t total) {
   off += align_up(size_t(k) * 8, 256);
   L.splits_off = off;
   off += align_up(size_t(L.num_tiles + 1) * k * 8, 256);
-  const size_t cn = size_t(L.num_coarse + 1);
-  L.c_splits_off = off;
-  off += L.coarse ? align_up(cn * k * 8, 256) : 0;
-  L.c_ub_off = off;
-  off += L.coarse ? align_up(cn * k * 8, 256) : 0;
-  L.c_lt_off = off;
-  off += L.coarse ? align_up(cn * k * 8, 256) : 0;
-  L.c_vstar_off = off;
-  off += L.coarse ? align_up(cn * sizeof(typename Tr::Bits), 256) : 0;
+  for (int l = 0; l < kBoundLevels; ++l) {
+    const u64 spacing = kTile * kBoundTiles[l];
+    const bool on = (k > 2) && (L.num_tiles > 2 * kBoundTiles[l]);
+    L.b_diag[l] = on ? (total + spacing - 1) / spacing + 1 : 0;
+    const size_t cn = size_t(L.b_diag[l]);
+    L.b_splits_off[l] = off;
+    off += align_up(cn * k * 8, 256);
+    L.b_ub_off[l] = off;
+    off += align_up(cn * k * 8, 256);
+    L.b_lt_off[l] = off;
+    off += align_up(cn * k * 8, 256);
+    L.b_vstar_off[l] = off;
+    off += align_up(cn * sizeof(typename Tr::Bits), 256);
+  }
   L.total = off;
   return L;
 }
@@ -544,7 +591,6 @@ cudaError_t kway_merge_typed(const void* const* runs_v, const size_t* lens, int 
   using Bits = typename Tr::Bits;
   if (k <= 0 || k > kMaxKwayRuns) return cudaErrorInvalidValue;
   const int shape = merge_shape(k);
-  const u64 kTile = merge_tile_keys(sizeof(Bits), shape);
   size_t total = 0;
   for (int r = 0; r < k; ++r) total += lens[r];
   if (total == 0) return cudaSuccess;
@@ -555,6 +601,7 @@ cudaError_t kway_merge_typed(const void* const* runs_v, const size_t* lens, int 
     return e;
   }
   const KwayLayout L = kway_layout<Tr>(k, total);
+  const u64 kTile = L.tile;
   if (temp == nullptr || temp_bytes < L.total) return cudaErrorInvalidValue;
   char* tb = static_cast<char*>(temp);
   const Bits** d_runs = reinterpret_cast<const Bits**>(tb + L.ptrs_off);
@@ -578,26 +625,29 @@ cudaError_t kway_merge_typed(const void* const* runs_v, const size_t* lens, int 
                       dim3(256), 0, stream, static_cast<const Bits*>(runs_v[0]), u64(lens[0]),
                       static_cast<const Bits*>(runs_v[1]), u64(lens[1]), kTile, num_diag, d_splits);
   } else {
+    // Bounding levels, coarsest first, each bounded by the one before; then every tile boundary.
     const u64* c_splits = nullptr;
     const u64* c_ub = nullptr;
     const u64* c_lt = nullptr;
     const Bits* c_vstar = nullptr;
-    const u64 c_spacing = kTile * kCoarseTiles;
-    if (L.coarse) {
-      u64* cs = reinterpret_cast<u64*>(tb + L.c_splits_off);
-      u64* cu = reinterpret_cast<u64*>(tb + L.c_ub_off);
-      u64* cl = reinterpret_cast<u64*>(tb + L.c_lt_off);
-      Bits* cv = reinterpret_cast<Bits*>(tb + L.c_vstar_off);
-      const u64 cdiag = L.num_coarse + 1;
+    u64 c_spacing = 1;
+    for (int l = 0; l < kBoundLevels; ++l) {
+      if (L.b_diag[l] == 0) continue;
+      u64* cs = reinterpret_cast<u64*>(tb + L.b_splits_off[l]);
+      u64* cu = reinterpret_cast<u64*>(tb + L.b_ub_off[l]);
+      u64* cl = reinterpret_cast<u64*>(tb + L.b_lt_off[l]);
+      Bits* cv = reinterpret_cast<Bits*>(tb + L.b_vstar_off[l]);
+      const u64 spacing = kTile * kBoundTiles[l];
+      const u64 cdiag = L.b_diag[l];
       e = launch_partition<Tr>(rec, k, dim3(unsigned((cdiag * 32 + 127) / 128)), stream, d_runs, d_lens, k,
-                               u64(total), c_spacing, cdiag, static_cast<const u64*>(nullptr),
-                               static_cast<const u64*>(nullptr), static_cast<const u64*>(nullptr),
-                               static_cast<const Bits*>(nullptr), u64(1), cs, cu, cl, cv);
+                               u64(total), spacing, cdiag, c_splits, c_ub, c_lt, c_vstar, c_spacing, cs, cu, cl,
+                               cv);
       if (e != cudaSuccess) return e;
       c_splits = cs;
       c_ub = cu;
       c_lt = cl;
       c_vstar = cv;
+      c_spacing = spacing;
     }
     e = launch_partition<Tr>(rec, k, dim3(unsigned((num_diag * 32 + 127) / 128)), stream, d_runs, d_lens, k,
                              u64(total), kTile, num_diag, c_splits, c_ub, c_lt, c_vstar, c_spacing, d_splits,
@@ -606,6 +656,23 @@ cudaError_t kway_merge_typed(const void* const* runs_v, const size_t* lens, int 
   if (e != cudaSuccess) return e;
   const Bits* const* cruns = d_runs;
   const u64* csplits = d_splits;
+  if (L.radix) {
+    // Output tiles in windows of about window_keys keys (one window when 0), as launch_tile_merges.
+    const u64 per_window =
+        window_keys == 0 ? L.num_tiles : std::max<u64>(1, (u64(window_keys) + kTile - 1) / kTile);
+    for (u64 t0 = 0; t0 < L.num_tiles; t0 += per_window) {
+      const u64 t1 = std::min<u64>(L.num_tiles, t0 + per_window);
+      e = kway_radix_tiles(dtype_of<Tr>(), cruns, k, reinterpret_cast<const uint64_t*>(d_splits), out, u64(total), t0,
+                           t1 - t0, stream, rec);
+      if (e != cudaSuccess) return e;
+      if (on_window) {
+        const u64 first = t0 * kTile, last = std::min<u64>(total, t1 * kTile);
+        e = on_window(size_t(first), size_t(last - first));
+        if (e != cudaSuccess) return e;
+      }
+    }
+    return cudaSuccess;
+  }
   switch (shape) {
     case 0:
       return launch_tile_merges<Tr, MergeShape<sizeof(Bits), 0>>(cruns, k, csplits, out, u64(total), L.num_tiles,

@@ -1221,6 +1221,145 @@ __global__ __launch_bounds__(kHistBlock, 1) void seg_histogram_kernel(const type
   }
 }
 
+// ---------------------------------------------------------------- K7c -------
+// One output tile of a stable k-way merge of 4-byte keys, sorted instead of
+// merged: the tile's slice of every run (from the split matrix) is staged back
+// to back in run order in shared memory, exactly as the pairwise-merge tiles
+// stage it, and then sorted by LSD passes over the ordered keys minus the
+// tile's smallest one. All of the tile's keys lie between the smallest slice
+// head and the largest slice tail, so ceil(bits(max - min) / 8) passes order
+// it (two for 16384 uniform keys out of 2^31). The passes are stable and the
+// staging order is run order, so equal keys keep the merge's order (lower run
+// first). Replaces the ceil(log2 k) pairwise rounds when k is large.
+template <class Tr, int BLOCK, int ITEMS, int MATCH>
+__global__ __launch_bounds__(BLOCK, 1) void kway_radix_tile_kernel(const typename Tr::Bits* const* __restrict__ runs,
+                                                                   int k, const unsigned long long* __restrict__ splits,
+                                                                   typename Tr::Bits* __restrict__ out,
+                                                                   unsigned long long total, unsigned long long tile0) {
+  using Bits = typename Tr::Bits;
+  using u64 = unsigned long long;
+  using Smem = OnesweepSmem<Tr, BLOCK, ITEMS, 1>;
+  static_assert(sizeof(Bits) == 4, "4-byte keys");
+  static_assert(sizeof(Smem) % 16 == 0, "run table after the sort buffers");
+  constexpr uint32_t kTile = uint32_t(BLOCK) * ITEMS;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  Smem& sm = *reinterpret_cast<Smem*>(smem_raw);
+  const Bits** sptr = reinterpret_cast<const Bits**>(smem_raw + sizeof(Smem));  // this tile's first key of every run
+  uint32_t* seg0 = reinterpret_cast<uint32_t*>(sptr + k);                        // slice offsets in the tile (k + 1)
+  __shared__ uint32_t scan_tmp[BLOCK / 32 + 1];
+  __shared__ uint32_t s_min, s_max;
+  const int tid = threadIdx.x;
+  const u64 j = tile0 + blockIdx.x;
+  const u64 d0 = j * u64(kTile);
+  const uint32_t cnt = uint32_t(min(u64(kTile), total - d0));
+  if (tid == 0) {
+    s_min = 0xFFFFFFFFu;
+    s_max = 0u;
+  }
+  for (int i = tid; i < Smem::kChains * 2 * kRadix; i += BLOCK) sm.masks[i] = 0u;
+
+  // Slice offsets (exclusive scan of the slice lengths) and the key range.
+  const int per_thread = (k + BLOCK - 1) / BLOCK;
+  uint32_t local = 0, lmin = 0xFFFFFFFFu, lmax = 0u;
+  for (int i = 0; i < per_thread; ++i) {
+    const int r = tid * per_thread + i;
+    if (r < k) {
+      const u64 s = splits[j * k + r], e = splits[(j + 1) * k + r];
+      sptr[r] = runs[r] + s;
+      local += uint32_t(e - s);
+      if (e > s) {
+        lmin = min(lmin, uint32_t(Tr::Ordered(runs[r][s])));
+        lmax = max(lmax, uint32_t(Tr::Ordered(runs[r][e - 1])));
+      }
+    }
+  }
+  uint32_t tot;
+  uint32_t run_off = block_exclusive_scan<BLOCK>(local, scan_tmp, &tot);
+  for (int i = 0; i < per_thread; ++i) {
+    const int r = tid * per_thread + i;
+    if (r < k) {
+      seg0[r] = run_off;
+      run_off += uint32_t(splits[(j + 1) * k + r] - splits[j * k + r]);
+    }
+  }
+  if (tid == 0) seg0[k] = cnt;
+  if (local) {
+    atomicMin(&s_min, lmin);
+    atomicMax(&s_max, lmax);
+  }
+  __syncthreads();
+
+  // Stage the slices back to back: consecutive threads read consecutive keys;
+  // every thread issues its loads before storing any, and its slice index
+  // only moves forward (its keys are BLOCK apart).
+  {
+    Bits v[ITEMS];
+    int r = 0;
+    {
+      int lo = 0, hi = k;  // largest r with seg0[r] <= tid
+      while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (seg0[mid] <= uint32_t(tid)) {
+          lo = mid;
+        } else {
+          hi = mid;
+        }
+      }
+      r = lo;
+    }
+    uint32_t r_end = seg0[r + 1];
+    const Bits* r_base = sptr[r] - seg0[r];
+#pragma unroll
+    for (int t = 0; t < ITEMS; ++t) {
+      const uint32_t i = uint32_t(t) * BLOCK + tid;
+      if (i < cnt) {
+        if (i >= r_end) {
+          do {
+            ++r;
+          } while (seg0[r + 1] <= i);  // seg0[k] = cnt > i ends the walk
+          r_end = seg0[r + 1];
+          r_base = sptr[r] - seg0[r];
+        }
+        v[t] = __ldg(r_base + i);
+      }
+    }
+#pragma unroll
+    for (int t = 0; t < ITEMS; ++t) {
+      const uint32_t i = uint32_t(t) * BLOCK + tid;
+      if (i < cnt) sm.keys[0][i] = v[t];
+    }
+  }
+  __syncthreads();
+
+  // Lean passes (the onesweep kernel's ranking: counters zero on entry, each
+  // warp clearing its own rows after its scatter); a full tile takes the
+  // fixed-span form, the last, shorter one spreads its keys over every warp.
+  const uint32_t range = cnt ? s_max - s_min : 0u;
+  const int passes = range == 0u ? 0 : (32 - __clz(int(range)) + 7) / 8;
+  const OffsetDigits dg{s_min};
+  const int warp = tid >> 5, lane = tid & 31;
+  for (int i = tid; i < Smem::kChains * kRadix; i += BLOCK) sm.ccount[i] = 0u;
+  __syncthreads();
+  int cur = 0;
+  for (int pass = 0; pass < passes; ++pass) {
+    uint32_t tc;
+    if (cnt == kTile) {
+      rank_tile<Tr, BLOCK, ITEMS, 1, MATCH, true, false, false, true>(
+          sm, sm.keys[cur], sm.keys[cur ^ 1], cnt, pass, &tc, [](uint32_t) {}, [](uint32_t) {},
+          static_cast<const NoValue*>(nullptr), static_cast<NoValue*>(nullptr), dg);
+    } else {
+      rank_tile<Tr, BLOCK, ITEMS, 1, MATCH, false, false, true, true>(
+          sm, sm.keys[cur], sm.keys[cur ^ 1], cnt, pass, &tc, [](uint32_t) {}, [](uint32_t) {},
+          static_cast<const NoValue*>(nullptr), static_cast<NoValue*>(nullptr), dg, (cnt + BLOCK - 1) / BLOCK);
+    }
+    for (int i = lane; i < kRadix; i += 32) sm.ccount[warp * kRadix + i] = 0u;
+    __syncthreads();
+    cur ^= 1;
+  }
+  Bits* o = out + d0;
+  for (uint32_t i = tid; i < cnt; i += BLOCK) o[i] = sm.keys[cur][i];
+}
+
 template <int P>
 __global__ __launch_bounds__(kRadix) void seg_scan_kernel(const uint32_t* __restrict__ counts,
                                                           const uint32_t* __restrict__ seg_hist,
@@ -1684,6 +1823,39 @@ cudaError_t segmented_sort_typed(typename Tr::Bits* keys, size_t n, const uint64
 }
 
 }  // namespace
+
+size_t kway_radix_tile_keys(int dtype) {
+  size_t keys = 0;
+  dispatch_dtype(dtype, [&](auto tr) {
+    using Tr = decltype(tr);
+    if constexpr (sizeof(typename Tr::Bits) == 4) keys = shape_tile<4, kDefaultShape>();
+  });
+  return keys;
+}
+
+cudaError_t kway_radix_tiles(int dtype, const void* d_runs, int k, const uint64_t* d_splits, void* out,
+                             uint64_t total, uint64_t tile0, uint64_t tiles, cudaStream_t stream,
+                             LaunchRecorder* rec) {
+  cudaError_t result = cudaErrorInvalidValue;
+  if (k < 1 || k > kMaxKwayTileRuns || tiles == 0 || tiles > 0x7FFFFFFFull) return result;
+  dispatch_dtype(dtype, [&](auto tr) {
+    using Tr = decltype(tr);
+    using Bits = typename Tr::Bits;
+    if constexpr (sizeof(Bits) == 4) {
+      using Shape = OnesweepShape<4, kDefaultShape>;
+      using Smem = OnesweepSmem<Tr, Shape::kBlock, Shape::kItems, 1>;
+      auto kernel = kway_radix_tile_kernel<Tr, Shape::kBlock, Shape::kItems, 3>;
+      static SmemLimitOnce attr;
+      result = attr.ensure(kernel, sizeof(Smem) + size_t(kMaxKwayTileRuns) * 12 + 4);
+      if (result != cudaSuccess) return;
+      result = launch_kernel(rec, "kway_radix_tiles", kernel, dim3(unsigned(tiles)), dim3(Shape::kBlock),
+                             sizeof(Smem) + size_t(k) * 12 + 4, stream, static_cast<const Bits* const*>(d_runs), k,
+                             reinterpret_cast<const unsigned long long*>(d_splits), static_cast<Bits*>(out),
+                             (unsigned long long)total, (unsigned long long)tile0);
+    }
+  });
+  return result;
+}
 
 cudaError_t set_wait_control(uint32_t lookback_spins, uint32_t tma_polls, uint32_t hold_tile) {
   const WaitControl wc{lookback_spins ? lookback_spins : kLookbackSpinLimit, tma_polls ? tma_polls : kTmaWaitLimit,

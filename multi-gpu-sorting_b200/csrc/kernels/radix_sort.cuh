@@ -62,7 +62,20 @@ cudaError_t radix_sort_range(int dtype, void* d_keys, void* d_values, size_t val
 cudaError_t radix_argsort(int dtype, void* d_keys, void* d_indices, size_t index_bytes, size_t n, void* d_temp,
                           size_t temp_bytes, cudaStream_t stream, uint32_t* d_status, LaunchRecorder* rec);
 
-// Number of kernel launches radix_sort issues for (dtype, n).
+// K-way merge tiles sorted in shared memory (the merge of many runs of 4-byte
+// keys): tile j in [tile0, tile0 + tiles) of the output is out[j*T, (j+1)*T)
+// (T = kway_radix_tile_keys(dtype), the last tile shorter), filled from the
+// slices splits[j*k + r] .. splits[(j+1)*k + r) of the k device runs (d_runs:
+// a device array of k run pointers; splits: a device (tiles+1) x k uint64
+// split matrix of a stable k-way merge at spacing T) by range-limited LSD
+// passes. kway_radix_tile_keys is 0 for dtypes without this path (8-byte keys).
+constexpr int kMaxKwayTileRuns = 1024;
+size_t kway_radix_tile_keys(int dtype);
+cudaError_t kway_radix_tiles(int dtype, const void* d_runs, int k, const uint64_t* d_splits, void* out,
+                             uint64_t total, uint64_t tile0, uint64_t tiles, cudaStream_t stream,
+                             LaunchRecorder* rec);
+
+// Number of kernel launches radix_sort issues for (dtype, n).// Number of kernel launches radix_sort issues for (dtype, n).
 int radix_sort_launches(int dtype, size_t n);
 
 // Onesweep variant choice. Key widths 4 and 8 bytes each have a table of

@@ -94,20 +94,24 @@ def test_kway_merge_matches_oracle(ctx, mgs, orc, dtype, k, total):
 
 
 @pytest.mark.parametrize("dtype", ["u32", "f32", "u64"])
-@pytest.mark.parametrize("pattern", ["empty-between", "tiny-many", "equal-keys"])
+@pytest.mark.parametrize("pattern", ["empty-between", "tiny-many", "equal-keys", "equal-keys-many"])
 def test_kway_merge_empty_and_tiny_runs(ctx, mgs, orc, dtype, pattern):
     """Empty slices between non-empty ones, many runs of one to three keys, and equal keys in every run
-    (ties must come out in run order): the per-tile pair walk of the merge rounds has to skip empty pairs."""
+    (ties must come out in run order): the per-tile pair walk of the merge rounds has to skip empty pairs.
+    "equal-keys-many" has enough runs for 4-byte keys to take the sorted-tile path (and a tile range of
+    zero: no pass at all)."""
     rng = np.random.default_rng(17)
     if pattern == "empty-between":
         lens = [0, 5, 0, 0, 3000, 0, 1, 0, 9000, 0, 0, 2, 0]
     elif pattern == "tiny-many":
         lens = list(rng.integers(0, 4, 1000))
-    else:
+    elif pattern == "equal-keys":
         lens = [4000, 0, 4001, 3, 4002, 0]
-    dist = "all-equal" if pattern == "equal-keys" else "full-uniform"
+    else:
+        lens = [int(x) for x in rng.integers(0, 3000, 40)]
+    dist = "all-equal" if pattern.startswith("equal-keys") else "full-uniform"
     runs = [orc.sort(keys(mgs, dtype, int(L), 31 + i, dist)) for i, L in enumerate(lens)]
-    if pattern == "equal-keys" and dtype == "f32":  # equal keys with different bytes: -0.0 / +0.0 by run
+    if pattern.startswith("equal-keys") and dtype == "f32":  # equal keys with different bytes: -0.0 / +0.0 by run
         runs = [np.full(int(L), -0.0 if i % 2 == 0 else 0.0, dtype=np.float32) for i, L in enumerate(lens)]
     total = int(sum(lens))
     want = orc.kway_merge(runs)
