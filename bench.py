@@ -586,7 +586,7 @@ def dirichlet_lengths(rng, k, total):
 
 def sweep_merge(mgs, torch, n, reps=3):
     """Chunked merge path (TanasicSort over g chunks of one GPU, g in 2, 4, 8) and the k-way merge of k in
-    2, 8, 32, 64 sorted runs with Dirichlet(1) lengths, n uint32 keys each."""
+    2, 8, 16, 32, 64 sorted runs with Dirichlet(1) lengths, n uint32 keys each."""
     ctx = mgs.Context(0)
     peak, _ = measured_hbm_peak()
     g = torch.Generator(device="cuda")
@@ -618,7 +618,7 @@ def sweep_merge(mgs, torch, n, reps=3):
     rng = np.random.default_rng(SEED)
     out = torch.empty_like(src)
     orc = None
-    for k in (2, 8, 32, 64):
+    for k in (2, 8, 16, 32, 64):
         lens = dirichlet_lengths(rng, k, n)
         offs = np.concatenate([[0], np.cumsum(lens)])
         runs = src.clone()
