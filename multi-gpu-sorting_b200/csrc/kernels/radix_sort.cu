@@ -522,7 +522,10 @@ __device__ __forceinline__ bool onesweep_tile(OnesweepSmem<Tr, BLOCK, ITEMS, CHA
   // earlier tiles of the segment, summing their aggregates until it meets an
   // inclusive prefix, with the statuses of kLookahead predecessors fetched per
   // round. With 512 threads the other eight warps rank their keys meanwhile, so
-  // the waits on other tiles overlap ranking.
+  // the waits on other tiles overlap ranking. A segment's first tile has no
+  // predecessor and its last tile places its keys from the bucket ends, so
+  // neither waits (in the segmented sort a short last tile would otherwise
+  // wait on its predecessor for most of a full tile's time).
   uint32_t tile_count = 0;
   const uint32_t warp_items = (SPREAD && !FULL) ? (valid + BLOCK - 1) / BLOCK : uint32_t(ITEMS);
   const int ranked = rank_tile<Tr, BLOCK, ITEMS, CHAINS, MATCH, FULL, false, SPREAD, true>(
@@ -534,7 +537,13 @@ __device__ __forceinline__ bool onesweep_tile(OnesweepSmem<Tr, BLOCK, ITEMS, CHA
       [&](uint32_t count) {
         if (tid >= kRadix) return;
         StatusT excl = 0;
-        if (tile > span.first_tile) {
+        if (tile > span.first_tile &&
+            (uint64_t(tile - span.first_tile) + 1u) * uint64_t(BLOCK * ITEMS) >= uint64_t(span.seg_len)) {
+          // The last tile of a segment (or of the array) needs no look-back: the digit totals of its span are
+          // known (the bucket starts), so its keys of digit d end the digit's bucket. No tile looks back at it.
+          const uint32_t end = tid + 1 < kRadix ? span.bucket[tid + 1] : span.seg_len;
+          excl = StatusT(end - span.bucket[tid] - count);
+        } else if (tile > span.first_tile) {
           const long long first = span.first_tile;
           long long jt = static_cast<long long>(tile) - 1;
           uint32_t spins = 0;
