@@ -76,6 +76,7 @@ MGS_SHAPE(8, 6, 512, 20, 1, 1)
 #undef MGS_SHAPE
 constexpr int kNumShapes = 7;
 constexpr int kDefaultShape = 5;
+constexpr int kSegShape = kDefaultShape;  // tile shape of the segmented sort's kernels
 
 constexpr int kHistBlock = 1024;
 constexpr int kHistUnroll = 4;
@@ -1047,7 +1048,7 @@ __device__ __forceinline__ void warp_sort_small(typename Tr::Bits* __restrict__ 
 // tiles).
 template <class Tr>
 constexpr uint32_t seg_small_cap() {
-  using Shape = OnesweepShape<sizeof(typename Tr::Bits), kDefaultShape>;
+  using Shape = OnesweepShape<sizeof(typename Tr::Bits), kSegShape>;
   return uint32_t(Shape::kItems) * 32u;
 }
 
@@ -1727,7 +1728,7 @@ struct SegLayout {
 template <class Tr>
 SegLayout seg_layout(size_t n, size_t nseg) {
   constexpr int w = int(sizeof(typename Tr::Bits));
-  constexpr size_t tile = shape_tile<w, kDefaultShape>();
+  constexpr size_t tile = shape_tile<w, kSegShape>();
   SegLayout L;
   L.max_large = std::min(nseg, n / (tile + 1) + 1);
   L.max_tiles = n / tile + L.max_large + 1;
@@ -1759,9 +1760,9 @@ cudaError_t segmented_sort_typed(typename Tr::Bits* keys, size_t n, const uint64
                                  void* temp, size_t temp_bytes, cudaStream_t stream, uint32_t* d_status,
                                  LaunchRecorder* rec) {
   using Bits = typename Tr::Bits;
-  using Shape = OnesweepShape<sizeof(Bits), kDefaultShape>;
+  using Shape = OnesweepShape<sizeof(Bits), kSegShape>;
   using Smem = OnesweepSmem<Tr, Shape::kBlock, Shape::kItems, Shape::kChains>;
-  constexpr uint32_t kTile = uint32_t(shape_tile<int(sizeof(Bits)), kDefaultShape>());
+  constexpr uint32_t kTile = uint32_t(shape_tile<int(sizeof(Bits)), kSegShape>());
   if (n == 0 || nseg == 0) return cudaSuccess;
   if (n >= (size_t(1) << 32) || nseg >= (size_t(1) << 32) - 1) return cudaErrorInvalidValue;
   const SegLayout L = seg_layout<Tr>(n, nseg);
