@@ -721,22 +721,17 @@ __global__ __launch_bounds__(BLOCK, MINB) void radix_onesweep_kernel(typename Tr
     if constexpr (kHasValues<V>) bulk_copy_g2s(sm.vals.v[b], w.v.start, w.v.bytes, &sm.bar[b]);
   };
 
-  // Persistent CTA: tiles come in launch order from an atomic counter. In the
-  // plain sort the leader claims one tile ahead of the one it prefetches: at
-  // the top of each iteration the tile claimed one iteration earlier becomes
-  // the next tile and the tile after it is claimed, a result first needed one
-  // iteration later (measured on 2^30 u32 keys: 0.6 % faster per pass). The
-  // segmented sort claims the next tile at the top of the iteration and loads
-  // its span record (claiming ahead measured 8 % slower there: its tiles,
-  // partial ones among them, take unequal times, and a tile claimed ahead
-  // waits behind two of its CTA's tiles while later tiles' look-backs wait
-  // for it). After the first barrier (every warp is past it, so the other
-  // buffer's previous tile is fully scattered) the leader works out the next
-  // tile's span and issues its TMA bulk copy into the other buffer, so loads
-  // overlap ranking. A CTA's current tile is older than its prefetched one,
-  // and that one older than its claimed one, so the oldest unfinished tile is
-  // always some CTA's current tile and the look-back makes progress.
-  constexpr bool kClaimAhead = !SEG;
+  // Persistent CTA: tiles come in launch order from an atomic counter. The
+  // leader claims the next tile at the top of each iteration and loads its
+  // span record (segmented sort); after the first barrier (every warp is past
+  // it, so the other buffer's previous tile is fully scattered) it works out
+  // the next tile's span and issues its TMA bulk copy into the other buffer,
+  // so loads overlap ranking. A CTA's current tile is always older than its
+  // prefetched one, so the oldest unfinished tile is always being processed
+  // and the look-back makes progress. (Claiming one tile further ahead made a
+  // lone 2^30-key sort 0.6 % faster but slowed sorts that share the GPU with
+  // others: in the serving loop it cut the full mix's peak from 28.2 to 24.4
+  // Gkeys/s and raised its p99 at 0.9 load from about 4 to 17-24 ms.)
   static_assert(sizeof(TileSpan<Tr>) <= sizeof(sm.span[0]), "span slot");
   TileSpan<Tr>* spans = reinterpret_cast<TileSpan<Tr>*>(sm.span);
   for (int i = tid; i < kChains * 2 * kRadix; i += BLOCK) sm.masks[i] = 0u;
@@ -745,7 +740,6 @@ __global__ __launch_bounds__(BLOCK, MINB) void radix_onesweep_kernel(typename Tr
   // warp (the first eight warps run the tile scan and the look-back; a
   // segment's tile span takes a few dependent loads).
   constexpr int kLeader = BLOCK - 32;
-  uint32_t claimed = num_tiles;  // leader, kClaimAhead: the tile claimed after the prefetched one
   if (tid == kLeader) {
     mbar_init(&sm.bar[0], 1);
     mbar_init(&sm.bar[1], 1);
@@ -753,7 +747,6 @@ __global__ __launch_bounds__(BLOCK, MINB) void radix_onesweep_kernel(typename Tr
     const uint32_t t = atomicAdd(&st->tile_counter[pass], 1u);
     sm.tile_id[0] = t;
     if (t < num_tiles) {
-      if (kClaimAhead) claimed = atomicAdd(&st->tile_counter[pass], 1u);
       const TileSpan<Tr> sp = span_of(record_of(t));
       spans[0] = sp;
       const Windows w = windows_of(sp, t);
@@ -770,12 +763,9 @@ __global__ __launch_bounds__(BLOCK, MINB) void radix_onesweep_kernel(typename Tr
     uint32_t next_tile = num_tiles;
     uint4 next_rec = make_uint4(0u, 0u, 0u, 0u);
     if (tid == kLeader) {
-      next_tile = kClaimAhead ? claimed : atomicAdd(&st->tile_counter[pass], 1u);
+      next_tile = atomicAdd(&st->tile_counter[pass], 1u);
       sm.tile_id[cur ^ 1] = next_tile;
-      if (next_tile < num_tiles) {
-        next_rec = record_of(next_tile);
-        if (kClaimAhead) claimed = atomicAdd(&st->tile_counter[pass], 1u);
-      }
+      if (next_tile < num_tiles) next_rec = record_of(next_tile);
     }
     auto issue_next = [&] {
       if (tid == kLeader && next_tile < num_tiles) {
