@@ -51,6 +51,19 @@ def test_sort_device_uniform_sizes(ctx, mgs, orc, dtype, n):
     assert device_sort(ctx, mgs, a, dtype).tobytes() == orc.sort(a).tobytes()
 
 
+@pytest.mark.parametrize("dtype,n", [
+    ("u32", 16384 * 300), ("u32", 16384 * 300 + 1),        # 2^22 <= n < 2^26: 16384-key tiles
+    ("f32", 16384 * 300 + 1), ("i64", 10240 * 500),        # 8-byte keys there: 10240-key tiles
+    ("u64", 10240 * 500 + 1),
+    ("u32", 20480 * 3300), ("u32", 20480 * 3300 + 1),      # n >= 2^26: 20480-key tiles
+])
+def test_sort_device_last_tile_full_or_one_key(ctx, mgs, orc, dtype, n):
+    """The array's last tile places its keys from the bucket ends instead of looking back: a last tile that
+    is full and one that holds a single key, for the tile sizes of the larger size classes."""
+    a = keys_for(mgs, dtype, "full-uniform", n, seed=23)
+    assert device_sort(ctx, mgs, a, dtype).tobytes() == orc.sort(a).tobytes()
+
+
 @pytest.mark.parametrize("dtype", TYPES)
 @pytest.mark.parametrize("dist", DISTS)
 @pytest.mark.parametrize("n", [5000, 300001])
