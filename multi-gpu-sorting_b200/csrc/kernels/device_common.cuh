@@ -81,15 +81,17 @@ struct RangeDigits {
   }
 };
 
-// Digits of the ordered key minus `base`, for 4-byte keys whose ordered values
-// all lie in [base, base + 2^(8 * passes)): a k-way merge tile whose keys span
-// a narrow range is sorted by that many passes.
+// Digits of the ordered key minus `base`, for keys whose ordered values all lie
+// in [base, base + 2^(8 * passes)): a set of keys that spans a narrow range (a
+// k-way merge tile, a segment) is sorted by that many passes. B is the key's
+// bit type.
+template <typename B>
 struct OffsetDigits {
-  uint32_t base;
+  B base;
   template <class Tr>
   __device__ __forceinline__ uint32_t digit(typename Tr::Bits k, int pass) const {
-    static_assert(sizeof(typename Tr::Bits) == 4, "4-byte keys");
-    return ((uint32_t(Tr::Ordered(k)) - base) >> (8 * pass)) & 0xFFu;
+    static_assert(sizeof(typename Tr::Bits) == sizeof(B), "base of the key's width");
+    return uint32_t((B(Tr::Ordered(k)) - base) >> (8 * pass)) & 0xFFu;
   }
 };
 

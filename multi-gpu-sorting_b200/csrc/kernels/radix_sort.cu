@@ -1061,8 +1061,10 @@ __global__ __launch_bounds__(BLOCK, MINB) void seg_small_medium_kernel(typename 
   extern __shared__ __align__(128) unsigned char smem_raw[];
   Smem& sm = *reinterpret_cast<Smem*>(smem_raw);
   __shared__ uint32_t s_work;
+  __shared__ Bits s_min[kWarps], s_max[kWarps];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   for (int i = tid; i < kChains * 2 * kRadix; i += BLOCK) sm.masks[i] = 0u;
+  for (int i = tid; i < kChains * kRadix; i += BLOCK) sm.ccount[i] = 0u;  // lean passes: zero on entry
   const uint32_t n_small = hdr->counts[0], n_medium = hdr->counts[1];
   for (;;) {
     __syncthreads();
@@ -1074,16 +1076,53 @@ __global__ __launch_bounds__(BLOCK, MINB) void seg_small_medium_kernel(typename 
     const unsigned long long b = offsets[seg];
     const uint32_t len = uint32_t(offsets[seg + 1] - b);
     Bits* g = keys + b;
-    for (uint32_t i = tid; i < len; i += BLOCK) sm.keys[0][i] = g[i];
+    // Load, with the range of the ordered keys: LSD passes over (ordered key - minimum), as many as the range's
+    // bits need, with the onesweep kernel's lean ranking (each warp clears its counter rows after its scatter).
+    Bits lo = ~Bits(0), hi = Bits(0);
+    for (uint32_t i = tid; i < len; i += BLOCK) {
+      const Bits k = g[i];
+      sm.keys[0][i] = k;
+      const Bits o = Tr::Ordered(k);
+      lo = o < lo ? o : lo;
+      hi = o > hi ? o : hi;
+    }
+#pragma unroll
+    for (int off = 16; off >= 1; off >>= 1) {
+      const Bits ol = __shfl_xor_sync(0xFFFFFFFFu, lo, off), oh = __shfl_xor_sync(0xFFFFFFFFu, hi, off);
+      lo = ol < lo ? ol : lo;
+      hi = oh > hi ? oh : hi;
+    }
+    if (lane == 0) {
+      s_min[warp] = lo;
+      s_max[warp] = hi;
+    }
+    __syncthreads();
+    lo = s_min[0];
+    hi = s_max[0];
+#pragma unroll
+    for (int w = 1; w < kWarps; ++w) {
+      lo = s_min[w] < lo ? s_min[w] : lo;
+      hi = s_max[w] > hi ? s_max[w] : hi;
+    }
+    const Bits range = hi - lo;  // len >= 2: lo <= hi
+    int bits = 0;
+    if constexpr (sizeof(Bits) == 4) {
+      bits = range ? 32 - __clz(int(range)) : 0;
+    } else {
+      bits = range ? 64 - __clzll((long long)range) : 0;
+    }
+    const int passes = (bits + 7) / 8;
+    const OffsetDigits<Bits> dg{lo};
     const uint32_t span = (len + BLOCK - 1) / BLOCK;  // keys per lane: every warp takes a share
     int cur = 0;
-    for (int pass = 0; pass < Tr::kPasses; ++pass) {
+    for (int pass = 0; pass < passes; ++pass) {
       uint32_t tc;
-      const bool skipped = rank_tile<Tr, BLOCK, ITEMS, CHAINS, MATCH, false, true, true>(
+      rank_tile<Tr, BLOCK, ITEMS, CHAINS, MATCH, false, false, true, true>(
           sm, sm.keys[cur], sm.keys[cur ^ 1], len, pass, &tc, [](uint32_t) {}, [](uint32_t) {},
-          static_cast<const NoValue*>(nullptr), static_cast<NoValue*>(nullptr), PlainDigits{}, span);
+          static_cast<const NoValue*>(nullptr), static_cast<NoValue*>(nullptr), dg, span);
+      for (int i = lane; i < kRadix; i += 32) sm.ccount[warp * kRadix + i] = 0u;
       __syncthreads();
-      if (!skipped) cur ^= 1;
+      cur ^= 1;
     }
     for (uint32_t i = tid; i < len; i += BLOCK) g[i] = sm.keys[cur][i];
   }
@@ -1336,7 +1375,7 @@ __global__ __launch_bounds__(BLOCK, 1) void kway_radix_tile_kernel(const typenam
   // fixed-span form, the last, shorter one spreads its keys over every warp.
   const uint32_t range = cnt ? s_max - s_min : 0u;
   const int passes = range == 0u ? 0 : (32 - __clz(int(range)) + 7) / 8;
-  const OffsetDigits dg{s_min};
+  const OffsetDigits<uint32_t> dg{s_min};
   const int warp = tid >> 5, lane = tid & 31;
   for (int i = tid; i < Smem::kChains * kRadix; i += BLOCK) sm.ccount[i] = 0u;
   __syncthreads();
