@@ -677,8 +677,8 @@ __global__ __launch_bounds__(BLOCK, MINB) void radix_onesweep_kernel(typename Tr
   Bits* dst = sel ? buf0 : buf1;
   const ValueSpan<V> vspan{sel ? vbuf1 : vbuf0, sel ? vbuf0 : vbuf1};
 
-  // A segmented tile's span comes from its 16-byte record (loaded ahead by the leader); a plain tile's span is
-  // the whole array.
+  // A segmented tile's span comes from its 16-byte record (loaded by the leader when it claims the tile); a
+  // plain tile's span is the whole array.
   auto span_of = [&](const uint4& rec) {
     if (SEG) {
       TileSpan<Tr> sp{src + rec.x, dst + rec.x, rec.z, rec.y,
@@ -738,7 +738,7 @@ __global__ __launch_bounds__(BLOCK, MINB) void radix_onesweep_kernel(typename Tr
   for (int i = tid; i < kChains * kRadix; i += BLOCK) sm.ccount[i] = 0u;  // then kept zero by each warp
   // The thread that claims tiles and issues their copies: a thread of the last
   // warp (the first eight warps run the tile scan and the look-back; a
-  // segment's tile span takes a few dependent loads).
+  // segmented tile's claim is followed by the load of its span record).
   constexpr int kLeader = BLOCK - 32;
   if (tid == kLeader) {
     mbar_init(&sm.bar[0], 1);
